@@ -1,0 +1,172 @@
+"""solve_batch and batch_summary over device tensors, through libgsb's C-ABI.
+
+solve_batch(X, S, prob, method, p=None; order, options, **kwargs) -> S      batched.jl:257-287
+solve_batch(X, prob, method, p=None; ...) -> ReturnCodeCounts               batched.jl:289-307
+Like the reference's `_launch!` (src/nonlinear/batched.jl:183-195) every call waits for its
+kernel before it returns. Host checks raise before any launch, with the reference's messages.
+"""
+
+from __future__ import annotations
+
+import ctypes
+
+from . import abi
+from .api import (
+    ArgumentError,
+    BatchSummary,
+    DimensionMismatch,
+    NonlinearProblem,
+    Options,
+    PerSystem,
+    ReturnCodeCounts,
+    SoA,
+    _raise_for,
+)
+
+
+def _tensor(x):
+    return x.data if isinstance(x, SoA) else x
+
+
+def _check_device_f64(t, what):
+    import torch
+
+    if not isinstance(t, torch.Tensor):
+        raise ArgumentError(f"{what} must be a torch tensor on a CUDA device")
+    if not t.is_cuda:
+        raise ArgumentError(f"{what} must be on a CUDA device (the batch solver has no host path)")
+    if t.dtype != torch.float64:
+        raise ArgumentError(f"{what} must be float64")
+    if not t.is_contiguous():
+        raise ArgumentError(f"{what} must be contiguous")
+
+
+def _resolve_options(options, kwargs):
+    """resolve_options, src/nonlinear/solver.jl:391-398: the keywords or an Options, never both."""
+    if options is None:
+        return Options(**kwargs)
+    if kwargs:
+        raise ArgumentError("pass either `options` or keyword arguments, not both")
+    if not isinstance(options, Options):
+        raise ArgumentError("options must be an Options")
+    return options
+
+
+def _is_perm(order, n):
+    import torch
+
+    o = order.detach().to("cpu", torch.int64)
+    if o.numel() != n:
+        return False
+    seen = torch.zeros(n, dtype=torch.bool)
+    if n == 0:
+        return True
+    if int(o.min()) < 0 or int(o.max()) >= n:
+        return False
+    seen[o] = True
+    return bool(seen.all())
+
+
+def solve_batch(X, S, prob=None, method=None, p=None, *, order=None, options=None, stream=None,
+                **kwargs):
+    """Solve every system of X in place (see the module docstring). X is an (nsys, n) float64
+    CUDA tensor (Vector{SVector}: one row per system) or SoA of an (n, nsys) tensor; S is a
+    (nsys, 72) uint8 tensor of statuses (``status_buffer``). `order` is a permutation of
+    0..nsys-1 (an int64 tensor on the device or host)."""
+    import torch
+
+    counts_form = isinstance(S, NonlinearProblem)
+    if counts_form:  # solve_batch(X, prob, method, p)
+        S, prob, method, p = None, S, prob, method
+    if not isinstance(prob, NonlinearProblem):
+        raise ArgumentError("prob must be a NonlinearProblem or a LeastSquaresProblem")
+    fam = prob.family
+    Xt = _tensor(X)
+    x_layout = abi.GSB_SOA if isinstance(X, SoA) else abi.GSB_AOS
+    _check_device_f64(Xt, "X")
+    if x_layout == abi.GSB_AOS:
+        if Xt.dim() != 2 or Xt.shape[1] != fam.n:
+            raise DimensionMismatch(f"X must be (nsys, {fam.n}), got {tuple(Xt.shape)}")
+        nsys = Xt.shape[0]
+    else:
+        if Xt.dim() != 2 or Xt.shape[0] != fam.n:
+            raise DimensionMismatch(f"SoA X must be ({fam.n}, nsys), got {tuple(Xt.shape)}")
+        nsys = Xt.shape[1]
+    # parameters: PerSystem only (the families take per-system data)
+    if not isinstance(p, PerSystem):
+        raise ArgumentError("p must be a PerSystem of per-system parameter blocks")
+    Pt = _tensor(p.data)
+    p_layout = abi.GSB_SOA if isinstance(p.data, SoA) else abi.GSB_AOS
+    _check_device_f64(Pt, "PerSystem data")
+    npar = fam.param_count
+    plen = Pt.shape[0] if p_layout == abi.GSB_AOS else (Pt.shape[1] if Pt.dim() == 2 else -1)
+    if Pt.dim() != 2 or plen != nsys:
+        raise DimensionMismatch(
+            f"PerSystem parameter length {plen} does not match batch length {nsys}")
+    if (Pt.shape[1] if p_layout == abi.GSB_AOS else Pt.shape[0]) != npar:
+        raise DimensionMismatch(f"each system takes {npar} parameters")
+    if Pt.device != Xt.device:
+        raise ArgumentError("PerSystem data must be on the device of X")
+    order_t = None
+    if order is not None:
+        order_t = torch.as_tensor(order)
+        if order_t.numel() != nsys:
+            raise DimensionMismatch(f"order length {order_t.numel()} does not match batch length {nsys}")
+        if not _is_perm(order_t, nsys):
+            raise ArgumentError(f"order is not a permutation of 0:{nsys - 1}")
+        order_t = order_t.to(device=Xt.device, dtype=torch.int64).contiguous()
+    opt = _resolve_options(options, kwargs)
+    if counts_form:
+        S_buf = torch.empty(nsys, dtype=torch.uint8, device=Xt.device)
+        s_kind = abi.GSB_CODES
+    else:
+        if not (isinstance(S, torch.Tensor) and S.dtype == torch.uint8 and S.is_cuda):
+            raise ArgumentError("S must be a (nsys, 72) uint8 CUDA tensor (status_buffer)")
+        if S.numel() != nsys * 72:
+            raise DimensionMismatch(
+                f"status vector length {S.numel() // 72} does not match batch length {nsys}")
+        if S.device != Xt.device:
+            raise ArgumentError(
+                f"status vector backend {S.device} does not match batch backend {Xt.device}")
+        S_buf = S
+        s_kind = abi.GSB_STATUS64
+    gm = method.to_abi()
+    if nsys == 0:
+        return ReturnCodeCounts(0, 0, 0, 0, 0, 0) if counts_form else S
+    lib = abi.load_library()
+    sh = prob.shared_device(Xt.device)
+    gp = prob.to_abi(None if sh is None else sh.data_ptr())
+    go = opt.to_abi()
+    if stream is None:
+        stream = torch.cuda.current_stream(Xt.device)
+    tally = abi.GsbTally()
+    with torch.cuda.device(Xt.device):
+        rc = lib.gsb_solve_batch(
+            ctypes.byref(gp), ctypes.byref(gm), ctypes.byref(go), Xt.data_ptr(), x_layout,
+            S_buf.data_ptr(), s_kind, Pt.data_ptr(), p_layout,
+            None if order_t is None else order_t.data_ptr(), 0, nsys,
+            ctypes.c_void_p(stream.cuda_stream), ctypes.byref(tally) if counts_form else None,
+        )
+        _raise_for(rc, lib)
+        _raise_for(lib.gsb_synchronize(ctypes.c_void_p(stream.cuda_stream)), lib)
+    if counts_form:
+        return ReturnCodeCounts(*[int(c) for c in tally.counts])
+    return S
+
+
+def batch_summary(S, stream=None) -> BatchSummary:
+    """batch_summary(S), src/nonlinear/batched.jl:80-89, reduced on the device."""
+    import torch
+
+    nsys = S.numel() // 72
+    if nsys == 0:
+        return BatchSummary(0.0, True, 0, 0, 0)
+    lib = abi.load_library()
+    if stream is None:
+        stream = torch.cuda.current_stream(S.device)
+    out = abi.GsbSummary()
+    with torch.cuda.device(S.device):
+        _raise_for(lib.gsb_batch_summary(S.data_ptr(), nsys, ctypes.c_void_p(stream.cuda_stream),
+                                         ctypes.byref(out)), lib)
+    return BatchSummary(out.fnorm, bool(out.all_converged), int(out.failure_count),
+                        int(out.max_iterations), int(out.total_iterations))

@@ -1,0 +1,234 @@
+/*
+ * gsb.h — the C-ABI of libgsb, a B200 (sm_100a) implementation of the R2 batched regime of
+ * GeometricSolvers.jl: many small independent nonlinear systems, one work item per system, one
+ * status per system.
+ *
+ * Reference interface replaced (paths are within the GeometricSolvers.jl project):
+ *   solve_batch!(X, S, prob, method, p; order, options, workgroupsize, kwargs...) -> S
+ *       src/nonlinear/batched.jl:257-287   -> gsb_solve_batch(..., s_kind = GSB_STATUS64)
+ *   solve_batch!(X, prob, method, p; ...) -> NamedTuple of the six ReturnCode counts
+ *       src/nonlinear/batched.jl:289-307   -> gsb_solve_batch(..., s_kind = GSB_CODES, tally)
+ *   batch_summary(S) -> BatchSummary
+ *       src/nonlinear/batched.jl:80-89     -> gsb_batch_summary
+ *   SolverStatus{Float64}   src/base/status.jl:101-117     -> GsbStatus64 (same byte layout)
+ *   Options{Float64}        src/base/options.jl:58-71      -> GsbOptions
+ *   ReturnCode              src/base/returncodes.jl:14     -> GsbReturnCode
+ *
+ * Conventions. Every call returns 0 on success and a negative GsbError otherwise; nothing aborts.
+ * Argument errors are detected on the host before any launch, as the reference's host checks
+ * (src/nonlinear/batched.jl:113-150, 270-283) are. Numerical failures are never errors: each is
+ * a GsbReturnCode in the status of its system. All array pointers are caller-owned DEVICE memory
+ * (CuArray, torch tensor, cudaMalloc) of the current device; `stream` is a cudaStream_t (NULL =
+ * the legacy default stream). Launches are stream-ordered; gsb_synchronize(stream) gives the
+ * blocking behaviour of the reference's `_launch!` (src/nonlinear/batched.jl:193).
+ */
+#ifndef GSB_H
+#define GSB_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GSB_ABI_VERSION 1
+
+/* ReturnCode, src/base/returncodes.jl:14 (UInt8, values 0..5 in this order). */
+typedef enum {
+    GSB_SUCCESS = 0,
+    GSB_STALLED = 1,
+    GSB_MAXITERS = 2,
+    GSB_SINGULAR = 3,
+    GSB_NONFINITE = 4,
+    GSB_LINESEARCH_FAILED = 5
+} GsbReturnCode;
+
+/* Host-side errors. They mirror the reference's ArgumentError / DimensionMismatch. */
+typedef enum {
+    GSB_OK = 0,
+    GSB_ERR_DIMENSION = -1,   /* DimensionMismatch: lengths that disagree */
+    GSB_ERR_ARGUMENT = -2,    /* ArgumentError: an invalid value or option */
+    GSB_ERR_UNSUPPORTED = -3, /* a combination the reference refuses or this build lacks */
+    GSB_ERR_CUDA = -4         /* a CUDA runtime error; gsb_last_error() has the text */
+} GsbError;
+
+/*
+ * SolverStatus{Float64} (src/base/status.jl:101-117) with Julia's field layout: offsets
+ * code 0, f_calls 2, iterations 4, fnorm 8, stepnorm 16, step_failures 24, promoted 28,
+ * stationary 29, jvp_calls 30, rank 32, nullnorm 40, gradratio 48, rate 56, contracted 64,
+ * reused 65; size 72, alignment 8. A Vector{SolverStatus{Float64}} is passed by pointer.
+ */
+typedef struct {
+    uint8_t code;
+    uint8_t pad0_;
+    int16_t f_calls;
+    int32_t iterations;
+    double fnorm;
+    double stepnorm;
+    int32_t step_failures;
+    uint8_t promoted;
+    uint8_t stationary;
+    int16_t jvp_calls;
+    int32_t rank;
+    uint32_t pad1_;
+    double nullnorm;
+    double gradratio;
+    double rate;
+    uint8_t contracted;
+    uint8_t reused;
+    uint8_t pad2_[6];
+} GsbStatus64;
+
+/* Options{Float64}, src/base/options.jl:58-71, field for field. Defaults :207-236. */
+typedef struct {
+    double f_abstol;
+    double f_reltol;
+    double x_abstol;
+    double x_reltol;
+    int32_t min_iterations;
+    int32_t max_iterations;
+    int32_t max_stalls;
+    int32_t norm; /* 0 = L2Norm, 1 = MaxNorm */
+    double g_tol;
+    double kappa;
+    uint8_t roundoff;
+    uint8_t rate_test;
+    uint8_t pad_[6];
+} GsbOptions;
+
+/* Residual families: device functions selected by this tag. */
+typedef enum {
+    /* F(x, p) = A x + 0.1 x.^3 - b, p = (A column-major n*n, b n); n in 1..32. */
+    GSB_FAMILY_CUBIC_AFFINE = 1,
+    /* Least squares r_i = sum_j a_j exp(-b_j t_i) - y_i, i = 1..m; x = (a1, b1, a2, b2, a3, b3),
+     * p = y (m values); the m abscissae t are the problem's shared constants. n = 6. */
+    GSB_FAMILY_EXPSUM3_LSQ = 2,
+    /* Gauss-Legendre 3-stage stage equations of the Henon-Heiles field: Z - h (A (x) I) f(y + Z)
+     * with x = Z the 12 stacked stage increments, p = y_n (q1, q2, p1, p2). Shared constants:
+     * h, then the 3x3 tableau A column-major. n = 12. */
+    GSB_FAMILY_IRK3_HENON_HEILES = 3,
+    /* Test families of the reference's batch tests, with analytic Jacobians (prob.J). */
+    GSB_FAMILY_HETERO6 = 100,  /* test/nonlinear/batched.jl:54-90; p = outcome 1..6; n = 2 */
+    GSB_FAMILY_COUPLED2 = 101  /* test/nonlinear/batched.jl:92-104; p = (p1, p2); n = 2 */
+} GsbFamily;
+
+typedef struct {
+    int32_t family;       /* GsbFamily */
+    int32_t n;            /* unknowns */
+    int32_t m;            /* residuals (m == n for a NonlinearProblem) */
+    int32_t pad_;
+    const double* shared; /* device pointer to the family's shared constants, or NULL */
+    int64_t shared_len;
+} GsbProblem;
+
+typedef enum { GSB_LU = 0, GSB_QR = 1 } GsbLinsolve;
+typedef enum { GSB_F64 = 0, GSB_F32 = 1 } GsbPrecision;
+typedef enum { GSB_NO_REFINEMENT = 0, GSB_REFINEMENT = 1 } GsbRefinementKind;
+typedef enum {
+    GSB_STATIC = 0,
+    GSB_BACKTRACKING = 1,
+    GSB_LEVENBERG_MARQUARDT = 2
+} GsbGlobalization;
+
+/*
+ * Newton (src/nonlinear/newton.jl:138-250) with the fields the batch path reads:
+ *   linsolve + factor_precision  = LUFactorization{TF}() / QRFactorization{TF}()
+ *   refinement                   = NoRefinement() / Refinement(eta, maxiter)
+ *   globalization                = Static(alpha) / Backtracking(c1, p, maxiter) /
+ *                                  LevenbergMarquardt(mu0, mu_min, mu_max, mu_decrease,
+ *                                                     mu_increase, rho_accept; scaling = :none)
+ * regularization must be 0 (the default); reuse, DogLeg and the matrix-free methods are not
+ * part of this ABI.
+ */
+typedef struct {
+    int32_t linsolve;         /* GsbLinsolve */
+    int32_t factor_precision; /* GsbPrecision */
+    int32_t refinement;       /* GsbRefinementKind */
+    int32_t refine_maxiter;
+    double refine_eta;
+    int32_t globalization;    /* GsbGlobalization */
+    int32_t bt_maxiter;
+    double static_alpha;
+    double bt_c1;
+    double bt_p;
+    double lm_mu0;
+    double lm_mu_min;
+    double lm_mu_max;
+    double lm_mu_decrease;
+    double lm_mu_increase;
+    double lm_rho_accept;
+    double regularization;
+} GsbMethod;
+
+/* The six counts of the count form, src/nonlinear/batched.jl:197-199, by GsbReturnCode. */
+typedef struct {
+    int64_t counts[6];
+} GsbTally;
+
+/* BatchSummary{Float64}, src/nonlinear/batched.jl:63-69. */
+typedef struct {
+    double fnorm;
+    int32_t all_converged;
+    int32_t max_iterations;
+    int64_t failure_count;
+    int64_t total_iterations;
+} GsbSummary;
+
+/* Layouts of X (nsys iterates of n values) and P (nsys parameter blocks). */
+typedef enum {
+    GSB_AOS = 0, /* entry k of system s at base[s * len + k]: Julia's Vector{SVector} */
+    GSB_SOA = 1  /* entry k of system s at base[k * nsys + s]: coalesced on the device */
+} GsbLayout;
+
+/* Forms of S. */
+typedef enum {
+    GSB_STATUS64 = 0, /* S is GsbStatus64[nsys] */
+    GSB_CODES = 1     /* S is uint8_t[nsys] ReturnCodes; the count form */
+} GsbStatusKind;
+
+/* ABI version and the sm_100a device code of this build (1 when compiled for sm_100a). */
+int gsb_abi_version(void);
+
+/* The last CUDA or argument error message of this thread, or "". */
+const char* gsb_last_error(void);
+
+/* Number of parameters per system of `prob` (n*n+n for GSB_FAMILY_CUBIC_AFFINE, ...), or a
+ * negative GsbError for an unknown family or size. */
+int64_t gsb_param_count(const GsbProblem* prob);
+
+/* Options(Float64) defaults, src/base/options.jl:207-236. */
+void gsb_default_options(GsbOptions* opt);
+
+/* Newton(; linsolve = LUFactorization(), globalization = Backtracking()) with the reference's
+ * defaults for every field (Backtracking c1 = 1e-4, p = 0.5, maxiter = 100; Static alpha = 1;
+ * Refinement eta = sqrt(eps), maxiter = 5; LevenbergMarquardt mu0 = 1e-6, mu_min = 1e-15,
+ * mu_max = 1e12, mu_decrease = 1/3, mu_increase = 4, rho_accept = 0). */
+void gsb_default_method(GsbMethod* method);
+
+/*
+ * Solve every system in place: X[idx] is the start of system idx and becomes its final iterate;
+ * S[idx] receives its status (s_kind GSB_STATUS64) or its code (GSB_CODES). P holds the
+ * per-system parameter blocks (PerSystem), in p_layout. When `order` is not NULL it is a
+ * permutation of 0..nsys-1 (order_base 0) or 1..nsys (order_base 1), and work item i solves
+ * system order[i] (src/nonlinear/batched.jl:91-92, 171-179); a non-permutation is
+ * GSB_ERR_ARGUMENT. When `tally` is not NULL (a host pointer) the call also returns the six
+ * counts, which synchronises `stream`. An empty batch returns at once (batched.jl:285, 303).
+ * Replaces solve_batch! (src/nonlinear/batched.jl:257-307).
+ */
+int gsb_solve_batch(const GsbProblem* prob, const GsbMethod* method, const GsbOptions* opt,
+                    double* X, int32_t x_layout, void* S, int32_t s_kind, const double* P,
+                    int32_t p_layout, const int64_t* order, int32_t order_base, int64_t nsys,
+                    void* stream, GsbTally* tally);
+
+/* batch_summary(S) of nsys device statuses into *out (host), src/nonlinear/batched.jl:80-89.
+ * Synchronises `stream`. */
+int gsb_batch_summary(const GsbStatus64* S, int64_t nsys, void* stream, GsbSummary* out);
+
+/* Wait for the work queued on `stream`. */
+int gsb_synchronize(void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GSB_H */

@@ -1,0 +1,490 @@
+"""Benchmark of the batch solver: systems solved per second at per-system relative error ≤ 1e-10
+with matching status codes, the chosen form against plain FP64, on the n = 8 cubic-affine batch
+of 1,048,576 systems (F(x) = A x + 0.1 x.^3 - b, A = 6I + 0.5 N(0,1), b ~ U(-1,1)^8, x0 = 0,
+f_abstol = 1e-12, f_reltol = 0, max_iterations = 50, Newton + LU + Backtracking).
+
+python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+A step solves one batch in place (the start iterates are copied into the working buffer, a
+device-to-device copy inside the step). The inputs (604 MB of parameters) exceed the 126 MB L2,
+so no flush is needed between steps. One JSON line is printed by rank 0.
+"""
+
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+
+N_UNKNOWNS = 8
+NSYS = 1 << 20
+METRIC = "systems solved/s at rel err ≤1e-10, chosen form vs plain FP64, one B200"
+REL_TOL = 1e-10
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="gsb200", choices=["gsb200", "reference"])
+    ap.add_argument("--nsys", type=int, default=NSYS)
+    ap.add_argument("--profile", choices=["plain", "mixed"], default=None,
+                    help="run `--warmup` + `--steps` solves of one form only (for ncu captures)")
+    return ap.parse_args()
+
+
+def options(gsb):
+    return gsb.Options(f_abstol=1e-12, f_reltol=0.0, max_iterations=50)
+
+
+def methods(gsb):
+    plain = gsb.Newton(globalization=gsb.Backtracking())
+    mixed = gsb.Newton(linsolve=gsb.LUFactorization("float32"), refinement=gsb.Refinement(),
+                       globalization=gsb.Backtracking())
+    return plain, mixed
+
+
+def workload(rank, nsys):
+    from workloads import cubic_affine
+
+    return cubic_affine(N_UNKNOWNS, nsys, 6.0, 1, stream=rank)
+
+
+# ─── roofline model ──────────────────────────────────────────────────────────────────────────
+
+
+def flops_per_system(n, iterations, f_evals):
+    """Floating-point operations of the plain FP64 Newton + LU + Backtracking step on the
+    cubic-affine family (a fused multiply-add counts 2, a division or square root 1), from the
+    oracle's per-system counts: f_evals residual evaluations (each with its merit) and
+    `iterations` steps (Jacobian, gradient ratio, pivoted LU, solve, step norms)."""
+    f_eval = 2 * n * n + 6 * n                       # rows, cubic terms, norm2
+    lu = n * (n - 1) // 2 + (n - 1) * n * (2 * n - 1) // 3
+    per_step = (6 * n                                  # forward-mode diagonal of J
+                + 4 * n * n + 2 * n + 4                # ‖J‖_F, Jᵀ F, their norms and ratio
+                + lu                                   # pivoted LU
+                + 2 * n * n - n                        # forward and back substitution
+                + 4 * n + 2 + 10)                      # ‖d‖, ‖x‖, the stopping tests
+    trials = np.maximum(f_evals - 1, 0)
+    return f_evals * f_eval + iterations * per_step + trials * 2 * n
+
+
+def bytes_per_system(n):
+    return 8 * n + 8 * (n * n + n) + 8 * n + 72
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    hbm = 6650.0
+    src = "fallback"
+    if os.path.exists(path):
+        with open(path) as fh:
+            hbm = float(json.load(fh)["hbm_gbs"])
+        src = "measured"
+    return hbm, src
+
+
+def fp_peaks():
+    lib = ctypes.CDLL(os.path.join(ROOT, "geometricsolvers.jl_b200", "peak", "libgsbpeak.so"))
+    lib.gsb_peak_fma.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+    out = {}
+    for name, fp64 in (("fp64", 1), ("fp32", 0)):
+        best = 0.0
+        for _ in range(3):
+            t = ctypes.c_double()
+            if lib.gsb_peak_fma(fp64, 4000, ctypes.byref(t)) == 0:
+                best = max(best, t.value)
+        out[name] = best
+    return out
+
+
+def profile_traffic():
+    """DRAM bytes per launch of the plain kernel from the committed ncu summary, if present."""
+    path = os.path.join(ROOT, "profiles", "newton_cubic8_fp64.md")
+    if not os.path.exists(path):
+        return None
+    with open(path) as fh:
+        for line in fh:
+            if line.startswith("traffic_bytes_per_launch_full:"):
+                return float(line.split(":", 1)[1])
+    return None
+
+
+# ─── clocks ──────────────────────────────────────────────────────────────────────────────────
+
+
+class Clocks:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join(ROOT, "_work", f"clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        os.makedirs(os.path.dirname(self.path), exist_ok=True)
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.fh, stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            self.proc.wait(timeout=10)
+            self.fh.close()
+
+    def summary(self):
+        if self.proc is None or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as fh:
+            for line in fh:
+                f = [v.strip() for v in line.split(",")]
+                if len(f) < 9:
+                    continue
+                try:
+                    sm.append(float(f[1]))
+                    smax.append(float(f[2]))
+                except ValueError:
+                    continue
+                for name, v in zip(names, f[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(name)
+        os.remove(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ─── the reference arm: the oracle (the CPU restatement) on the host cores ─────────────────
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    import gsb200 as G
+    from oracle import oracle_py as O
+
+    nt = O.max_threads()
+    X0, P = workload(0, args.nsys)
+    prob = G.NonlinearProblem(G.CubicAffine(N_UNKNOWNS))
+    plain, _ = methods(G)
+    opts = options(G)
+    sample = min(args.nsys, 262144)
+    times = []
+    for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        O.solve_batch(prob, plain, X0[:sample].copy(), P[:sample], opts, nthreads=nt)
+        dt = time.perf_counter() - t0
+        if i >= args.warmup:
+            times.append(dt)
+    med = statistics.median(times)
+    value = sample / med
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "systems/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": med * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Philox)",
+        "config": {"workload": f"cubic-affine n=8, {args.nsys} systems, Newton+LU+Backtracking FP64",
+                   "sample_systems": sample},
+        "cpu_baseline": {"value": value, "unit": "systems/s", "cores": nt, "kind": "port",
+                         "sample": f"{sample} of the {args.nsys} systems per step, plain FP64"},
+        "e2e": {"value": value, "unit": "systems/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ─── our arm ─────────────────────────────────────────────────────────────────────────────────
+
+
+def rel_err(x, xr):
+    num = np.max(np.abs(x - xr), axis=1)
+    den = np.max(np.abs(xr), axis=1)
+    with np.errstate(invalid="ignore", divide="ignore"):
+        return np.where(den > 0, num / den, num)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+    if args.profile:
+        run_profile(args)
+        return
+
+    import torch
+    import torch.distributed as dist
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(v):
+        if world == 1:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum_over_ranks(v):
+        if world == 1:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        return float(t.item())
+
+    import gsb200 as G
+    from oracle import oracle_py as O
+
+    nsys = args.nsys
+    X0_h, P_h = workload(rank, nsys)
+    prob = G.NonlinearProblem(G.CubicAffine(N_UNKNOWNS))
+    plain, mixed = methods(G)
+    opts = options(G)
+    X0 = torch.tensor(X0_h, device=dev)
+    P = torch.tensor(P_h, device=dev)
+    X = torch.empty_like(X0)
+    S = G.status_buffer(nsys, device=dev)
+    ps = G.PerSystem(P)
+    stream = torch.cuda.current_stream(dev)
+
+    # correctness of each form against the oracle (untimed): the count of systems solved
+    nt = max(1, O.max_threads() // max(1, world))
+    xo, so = O.solve_batch(prob, plain, X0_h.copy(), P_h, opts, nthreads=nt)
+    solved = {}
+    fp64_err = {}
+    for name, m in (("plain_fp64", plain), ("fp32_lu_refinement", mixed)):
+        X.copy_(X0)
+        G.solve_batch(X, S, prob, m, ps, options=opts)
+        st = G.statuses(S)
+        x = X.cpu().numpy()
+        err = rel_err(x, xo)
+        ok = (st["code"] == so["code"]) & (err <= REL_TOL)
+        solved[name] = int(np.count_nonzero(ok))
+        fp64_err[name] = float(np.max(err))
+        if name == "plain_fp64":
+            iters_match = bool(np.array_equal(st["iterations"], so["iterations"]))
+    flops = float(np.sum(flops_per_system(N_UNKNOWNS, so["iterations"].astype(np.int64),
+                                          so["iterations"].astype(np.int64) * 0 + 1 +
+                                          _trials(so))))
+
+    def timed(m, steps, warmup):
+        for _ in range(warmup):
+            X.copy_(X0)
+            G.solve_batch(X, S, prob, m, ps, options=opts)
+        barrier()
+        torch.cuda.synchronize(dev)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            X.copy_(X0)
+            G.solve_batch(X, S, prob, m, ps, options=opts)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        barrier()
+        return max_over_ranks(e0.elapsed_time(e1) / steps)
+
+    # kernel-only time of one launch (no copy), for the roofline
+    def kernel_ms(m, reps=5):
+        ts = []
+        for _ in range(reps):
+            X.copy_(X0)
+            torch.cuda.synchronize(dev)
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            G.solve_batch(X, S, prob, m, ps, options=opts)
+            b.record(stream)
+            torch.cuda.synchronize(dev)
+            ts.append(a.elapsed_time(b))
+        return statistics.median(ts)
+
+    with Clocks(local) as clk:
+        ms_plain = timed(plain, args.steps, args.warmup)
+        ms_mixed = timed(mixed, args.steps, args.warmup)
+    clocks = clk.summary()
+    chosen_name = "fp32_lu_refinement" if solved["fp32_lu_refinement"] / ms_mixed >= \
+        solved["plain_fp64"] / ms_plain else "plain_fp64"
+    chosen_m = mixed if chosen_name == "fp32_lu_refinement" else plain
+    ms_chosen = ms_mixed if chosen_name == "fp32_lu_refinement" else ms_plain
+    total_solved = sum_over_ranks(solved[chosen_name])
+    value = total_solved / (ms_chosen * 1e-3)
+    plain_value = sum_over_ranks(solved["plain_fp64"]) / (ms_plain * 1e-3)
+
+    # end to end through the public API: pinned host inputs in, results out, every step
+    x0_pin = torch.from_numpy(X0_h).pin_memory()
+    p_pin = torch.from_numpy(P_h).pin_memory()
+    x_out = torch.empty_like(x0_pin).pin_memory()
+    s_out = torch.empty((nsys, 72), dtype=torch.uint8).pin_memory()
+    Xe = torch.empty_like(X0)
+    Pe = torch.empty_like(P)
+    pse = G.PerSystem(Pe)
+
+    def e2e_step():
+        Xe.copy_(x0_pin, non_blocking=True)
+        Pe.copy_(p_pin, non_blocking=True)
+        G.solve_batch(Xe, S, prob, chosen_m, pse, options=opts)
+        x_out.copy_(Xe, non_blocking=True)
+        s_out.copy_(S, non_blocking=True)
+
+    for _ in range(max(1, args.warmup // 2)):
+        e2e_step()
+    torch.cuda.synchronize(dev)
+    barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e2e_steps = max(1, args.steps // 2)
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        e2e_step()
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    barrier()
+    ms_e2e = max_over_ranks(e0.elapsed_time(e1) / e2e_steps)
+    e2e_value = total_solved / (ms_e2e * 1e-3)
+    h2d = X0_h.nbytes + P_h.nbytes
+    d2h = X0_h.nbytes + nsys * 72
+
+    # roofline of the plain FP64 kernel
+    hbm_peak, hbm_src = measured_peaks()
+    peaks = fp_peaks()
+    kms = kernel_ms(plain)
+    bytes_total = bytes_per_system(N_UNKNOWNS) * nsys
+    t_bytes = bytes_total / (hbm_peak * 1e9)
+    t_flops = flops / (peaks["fp64"] * 1e12)
+    achieved_gbs = bytes_total / (kms * 1e-3) / 1e9
+    achieved_tf = flops / (kms * 1e-3) / 1e12
+    traffic = profile_traffic()
+    if t_bytes >= t_flops:
+        roof = {"bound": "hbm", "achieved": achieved_gbs, "peak": hbm_peak, "unit": "GB/s",
+                "frac": achieved_gbs / hbm_peak, "traffic": traffic,
+                "peak_source": f"{hbm_src} (MEASURED_PEAKS.json hbm_gbs)"}
+    else:
+        roof = {"bound": "fp64", "achieved": achieved_tf, "peak": peaks["fp64"],
+                "unit": "TFLOP/s", "frac": achieved_tf / peaks["fp64"], "traffic": traffic,
+                "peak_source": "measured (FP64 FMA probe, libgsbpeak)"}
+    roof["kernel"] = "newton_kernel<CubicAffine<8>, fused, FP64>"
+    roof["kernel_ms"] = kms
+    roof["fp64_frac"] = achieved_tf / peaks["fp64"] if peaks["fp64"] else None
+    roof["hbm_frac"] = achieved_gbs / hbm_peak
+    roof["flops_per_launch"] = flops
+    roof["bytes_per_launch"] = bytes_total
+    roof["fp64_peak_tflops"] = peaks["fp64"]
+    roof["fp32_peak_tflops"] = peaks["fp32"]
+
+    # CPU baseline: the oracle on the host cores, on a bounded sample of the same batch
+    cpu = None
+    if rank == 0 and world == 1:
+        ntall = O.max_threads()
+        sample = 262144
+        reps, t_tot = 0, 0.0
+        while t_tot < 10.0 and reps < 40:
+            t0 = time.perf_counter()
+            O.solve_batch(prob, plain, X0_h[:sample].copy(), P_h[:sample], opts, nthreads=ntall)
+            t_tot += time.perf_counter() - t0
+            reps += 1
+        cpu = {"value": sample * reps / t_tot, "unit": "systems/s", "cores": ntall, "kind": "port",
+               "sample": f"{reps} x {sample} of the {nsys} systems, plain FP64, "
+                         f"{ntall} threads, {t_tot:.1f} s"}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "systems/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_chosen,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded Philox; reference configuration's shapes and distributions)",
+        "config": {
+            "workload": "cubic-affine F = A x + 0.1 x.^3 - b, n=8, 1,048,576 systems per GPU, "
+                        "Newton + LU + Backtracking, f_abstol 1e-12, max_iterations 50",
+            "chosen_form": chosen_name, "global_batch": int(nsys * world),
+            "parallelism": f"independent shards x{world} (no collective in the solve)",
+            "l2": "inputs (604 MB parameters) exceed the 126 MB L2; no flush",
+        },
+        "forms": {
+            "plain_fp64": {"systems_per_s": plain_value, "ms_per_step": ms_plain,
+                           "solved": solved["plain_fp64"], "fp64_oracle_max_rel_err": fp64_err["plain_fp64"],
+                           "iterations_match_oracle": iters_match},
+            "fp32_lu_refinement": {"systems_per_s": sum_over_ranks(solved["fp32_lu_refinement"]) / (ms_mixed * 1e-3),
+                                   "ms_per_step": ms_mixed, "solved": solved["fp32_lu_refinement"],
+                                   "fp64_oracle_max_rel_err": fp64_err["fp32_lu_refinement"]},
+            "chosen_over_plain": value / plain_value,
+        },
+        "e2e": {"value": e2e_value, "unit": "systems/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e},
+        "gpu_launches": args.steps,
+        "roofline": roof,
+        "cpu_baseline": cpu,
+        "clocks": clocks,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def run_profile(args):
+    """Solves of one form on args.nsys systems, for an ncu capture of the batch kernel."""
+    import torch
+
+    import gsb200 as G
+
+    X0_h, P_h = workload(0, args.nsys)
+    prob = G.NonlinearProblem(G.CubicAffine(N_UNKNOWNS))
+    plain, mixed = methods(G)
+    m = plain if args.profile == "plain" else mixed
+    X0 = torch.tensor(X0_h, device="cuda")
+    P = G.PerSystem(torch.tensor(P_h, device="cuda"))
+    X = torch.empty_like(X0)
+    S = G.status_buffer(args.nsys)
+    for _ in range(args.warmup + args.steps):
+        X.copy_(X0)
+        G.solve_batch(X, S, prob, m, P, options=options(G))
+    torch.cuda.synchronize()
+    st = G.statuses(S)
+    print(json.dumps({"profile": args.profile, "nsys": args.nsys,
+                      "codes": np.bincount(st["code"], minlength=6).tolist()}))
+
+
+def _trials(so):
+    """Line-search trials per system are not in the status; the flop model takes one trial per
+    step (the accepted full step of a converging Newton iteration)."""
+    return so["iterations"].astype(np.int64)
+
+
+if __name__ == "__main__":
+    main()

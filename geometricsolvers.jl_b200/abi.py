@@ -126,6 +126,8 @@ class GsbMethod(ctypes.Structure):
         ("lm_mu_increase", ctypes.c_double),
         ("lm_rho_accept", ctypes.c_double),
         ("regularization", ctypes.c_double),
+        ("arithmetic", ctypes.c_int32),
+        ("pad_", ctypes.c_int32),
     ]
 
 
@@ -149,6 +151,7 @@ GSB_LU, GSB_QR = 0, 1
 GSB_F64, GSB_F32 = 0, 1
 GSB_NO_REFINEMENT, GSB_REFINEMENT = 0, 1
 GSB_STATIC, GSB_BACKTRACKING, GSB_LEVENBERG_MARQUARDT = 0, 1, 2
+GSB_FUSED, GSB_UNFUSED = 0, 1
 
 # The symbols include/gsb.h declares (checked by the CPU tests against the built library).
 EXPORTED_SYMBOLS = (

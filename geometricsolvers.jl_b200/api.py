@@ -213,8 +213,13 @@ class Newton:
     refinement: object = NoRefinement()
     regularization: float = 0.0
     reuse: Optional[int] = None
+    # The rounding of the linear algebra on the device: "fused" (FMA, the default) or
+    # "unfused" (every product and sum rounded alone, as Julia evaluates); no reference field.
+    arithmetic: str = "fused"
 
     def __post_init__(self):
+        if self.arithmetic not in ("fused", "unfused"):
+            raise ArgumentError("arithmetic must be 'fused' or 'unfused'")
         if isinstance(self.refinement, bool):
             object.__setattr__(self, "refinement", Refinement() if self.refinement else NoRefinement())
         if not (self.regularization >= 0 and math.isfinite(self.regularization)):
@@ -268,6 +273,7 @@ class Newton:
         if self.reuse is not None:
             raise ArgumentError("the batch path takes no factor reuse")
         m.regularization = 0.0
+        m.arithmetic = abi.GSB_FUSED if self.arithmetic == "fused" else abi.GSB_UNFUSED
         return m
 
 

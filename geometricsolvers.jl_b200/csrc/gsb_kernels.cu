@@ -1,0 +1,391 @@
+// libgsb: the batch kernels and the C-ABI of include/gsb.h.
+//
+// One launch solves a batch: one thread per system (the work item of the reference's
+// `_solve_kernel!`, src/nonlinear/batched.jl:171-179). A CTA first stages the parameter blocks
+// of its systems into shared memory (coalesced loads of the CTA's contiguous AoS chunk, or one
+// coalesced load per entry for SoA), each system's block in a row of odd stride so that the
+// per-thread reads are free of bank conflicts; then each thread runs its solve in registers and
+// writes its iterate and its 72-byte status.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/gsb.h"
+#include "gsb_kernel_impl.cuh"
+
+namespace gsb {
+
+// batch_summary partials: Σ fnorm², max |fnorm|, failures, max and Σ iterations.
+struct SummaryAcc {
+    double sumsq;
+    unsigned long long maxbits;  // bits of max |fnorm| (non-negative doubles order as integers)
+    unsigned long long failures;
+    unsigned long long total_iterations;
+    int max_iterations;
+    int nan_seen;
+};
+
+__global__ void summary_kernel(const unsigned char* S, int64_t nsys, SummaryAcc* acc, int scale_e,
+                               int pass) {
+    double sq = 0.0;
+    unsigned long long mb = 0, fails = 0, tot = 0;
+    int mx = 0, nan = 0;
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < nsys;
+         q += (int64_t)gridDim.x * blockDim.x) {
+        const unsigned char* st = S + q * 72;
+        int code = st[0];
+        int it = *reinterpret_cast<const int*>(st + 4);
+        double fn = *reinterpret_cast<const double*>(st + 8);
+        if (pass == 0) {
+            sq = __fma_rn(fn, fn, sq);
+            unsigned long long b = (unsigned long long)__double_as_longlong(fabs(fn));
+            if (fn != fn) nan = 1;
+            mb = b > mb ? b : mb;
+            fails += code != SUCCESS;
+            tot += (unsigned long long)it;
+            mx = it > mx ? it : mx;
+        } else {
+            double u = ldexp2(fn, -scale_e);
+            sq = __fma_rn(u, u, sq);
+        }
+    }
+    for (int off = 16; off; off >>= 1) {
+        sq += __shfl_xor_sync(0xffffffffu, sq, off);
+        unsigned long long ob = __shfl_xor_sync(0xffffffffu, mb, off);
+        mb = ob > mb ? ob : mb;
+        fails += __shfl_xor_sync(0xffffffffu, fails, off);
+        tot += __shfl_xor_sync(0xffffffffu, tot, off);
+        int om = __shfl_xor_sync(0xffffffffu, mx, off);
+        mx = om > mx ? om : mx;
+        nan |= __shfl_xor_sync(0xffffffffu, nan, off);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(&acc->sumsq, sq);
+        if (pass == 0) {
+            atomicMax(&acc->maxbits, mb);
+            atomicAdd(&acc->failures, fails);
+            atomicAdd(&acc->total_iterations, tot);
+            atomicMax(&acc->max_iterations, mx);
+            atomicOr(&acc->nan_seen, nan);
+        }
+    }
+}
+
+}  // namespace gsb
+
+using namespace gsb;
+
+// ─── host side ──────────────────────────────────────────────────────────────────────────────
+
+namespace {
+
+thread_local std::string g_err;
+
+int set_err(int code, const std::string& msg) {
+    g_err = msg;
+    return code;
+}
+
+int cuda_err(cudaError_t e, const char* where) {
+    if (e == cudaSuccess) return 0;
+    return set_err(GSB_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+// Per-device workspace: the tally counters and the summary accumulator.
+struct Workspace {
+    unsigned long long* tally = nullptr;
+    SummaryAcc* acc = nullptr;
+};
+std::mutex g_ws_mu;
+Workspace g_ws[64];
+
+int workspace(Workspace** out) {
+    int dev = 0;
+    if (int rc = cuda_err(cudaGetDevice(&dev), "cudaGetDevice")) return rc;
+    if (dev < 0 || dev >= 64) return set_err(GSB_ERR_CUDA, "device index out of range");
+    std::lock_guard<std::mutex> lk(g_ws_mu);
+    Workspace& w = g_ws[dev];
+    if (!w.tally) {
+        if (int rc = cuda_err(cudaMalloc(&w.tally, 6 * sizeof(unsigned long long)), "cudaMalloc"))
+            return rc;
+        if (int rc = cuda_err(cudaMalloc(&w.acc, sizeof(SummaryAcc)), "cudaMalloc")) return rc;
+    }
+    *out = &w;
+    return 0;
+}
+
+int64_t param_count(const GsbProblem* p) {
+    switch (p->family) {
+    case GSB_FAMILY_CUBIC_AFFINE:
+        return (p->n >= 1 && p->n <= 32) ? (int64_t)p->n * p->n + p->n : GSB_ERR_ARGUMENT;
+    case GSB_FAMILY_EXPSUM3_LSQ: return p->m;
+    case GSB_FAMILY_IRK3_HENON_HEILES: return 4;
+    case GSB_FAMILY_HETERO6: return 1;
+    case GSB_FAMILY_COUPLED2: return 2;
+    default: return GSB_ERR_ARGUMENT;
+    }
+}
+
+}  // namespace
+
+namespace gsb {
+GSB_DECLARE_ENTRY(cubic2);
+GSB_DECLARE_ENTRY(cubic3);
+GSB_DECLARE_ENTRY(cubic4);
+GSB_DECLARE_ENTRY(cubic6);
+GSB_DECLARE_ENTRY(cubic8);
+GSB_DECLARE_ENTRY(hetero6);
+GSB_DECLARE_ENTRY(coupled2);
+}  // namespace gsb
+
+namespace {
+
+KernelEntry* select_kernel(const GsbProblem* prob, bool fused, bool mixed) {
+    switch (prob->family) {
+    case GSB_FAMILY_CUBIC_AFFINE:
+        switch (prob->n) {
+        case 2: return entry_cubic2(fused, mixed);
+        case 3: return entry_cubic3(fused, mixed);
+        case 4: return entry_cubic4(fused, mixed);
+        case 6: return entry_cubic6(fused, mixed);
+        case 8: return entry_cubic8(fused, mixed);
+        default: return nullptr;
+        }
+    case GSB_FAMILY_HETERO6: return entry_hetero6(fused, mixed);
+    case GSB_FAMILY_COUPLED2: return entry_coupled2(fused, mixed);
+    default: return nullptr;
+    }
+}
+
+bool nonneg(double v) { return v >= 0.0; }
+
+int check_options(const GsbOptions* o) {
+    if (!(nonneg(o->f_abstol) && nonneg(o->f_reltol) && nonneg(o->x_abstol) &&
+          nonneg(o->x_reltol) && nonneg(o->g_tol)))
+        return set_err(GSB_ERR_ARGUMENT, "tolerances must be non-negative");
+    if (o->min_iterations < 0) return set_err(GSB_ERR_ARGUMENT, "min_iterations must be non-negative");
+    if (o->max_iterations < o->min_iterations)
+        return set_err(GSB_ERR_ARGUMENT, "max_iterations is below min_iterations");
+    if (o->max_stalls < 1) return set_err(GSB_ERR_ARGUMENT, "max_stalls must be at least 1");
+    if (!(o->kappa > 0.0 && o->kappa < 1.0))
+        return set_err(GSB_ERR_ARGUMENT, "kappa must be finite and in (0, 1)");
+    if (o->norm != 0 && o->norm != 1) return set_err(GSB_ERR_ARGUMENT, "norm must be L2 or Max");
+    return 0;
+}
+
+int check_method(const GsbMethod* m) {
+    if (m->linsolve != GSB_LU && m->linsolve != GSB_QR)
+        return set_err(GSB_ERR_ARGUMENT, "linsolve must be LU or QR");
+    if (m->factor_precision != GSB_F64 && m->factor_precision != GSB_F32)
+        return set_err(GSB_ERR_ARGUMENT, "factor precision must be F64 or F32");
+    if (m->globalization < GSB_STATIC || m->globalization > GSB_LEVENBERG_MARQUARDT)
+        return set_err(GSB_ERR_ARGUMENT, "unknown globalization");
+    if (m->globalization == GSB_STATIC && !(m->static_alpha > 0.0 && isfinite(m->static_alpha)))
+        return set_err(GSB_ERR_ARGUMENT, "the step of Static must be positive and finite");
+    if (m->globalization == GSB_BACKTRACKING &&
+        !(m->bt_c1 > 0 && m->bt_c1 < 1 && m->bt_p > 0 && m->bt_p < 1 && m->bt_maxiter >= 1))
+        return set_err(GSB_ERR_ARGUMENT, "Backtracking needs 0 < c1 < 1, 0 < p < 1, maxiter >= 1");
+    if (m->refinement == GSB_REFINEMENT &&
+        !(m->refine_maxiter >= 1 && m->refine_eta > 0 && m->refine_eta < 1))
+        return set_err(GSB_ERR_ARGUMENT, "Refinement needs maxiter >= 1 and 0 < eta < 1");
+    if (m->globalization == GSB_LEVENBERG_MARQUARDT && m->refinement == GSB_REFINEMENT)
+        return set_err(GSB_ERR_UNSUPPORTED,
+                       "Newton with a LevenbergMarquardt globalization takes no refinement");
+    if (m->regularization != 0.0)
+        return set_err(GSB_ERR_UNSUPPORTED, "the batch path takes regularization = 0");
+    if (m->arithmetic != GSB_FUSED && m->arithmetic != GSB_UNFUSED)
+        return set_err(GSB_ERR_ARGUMENT, "arithmetic must be GSB_FUSED or GSB_UNFUSED");
+    return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int gsb_abi_version(void) { return GSB_ABI_VERSION; }
+
+const char* gsb_last_error(void) { return g_err.c_str(); }
+
+int64_t gsb_param_count(const GsbProblem* prob) {
+    if (!prob) return GSB_ERR_ARGUMENT;
+    return param_count(prob);
+}
+
+void gsb_default_options(GsbOptions* o) {
+    std::memset(o, 0, sizeof(*o));
+    o->f_abstol = 0.0;
+    o->f_reltol = 1.4901161193847656e-08;
+    o->x_abstol = 0.0;
+    o->x_reltol = 2.0 * 2.220446049250313e-16;
+    o->min_iterations = 0;
+    o->max_iterations = 100;
+    o->max_stalls = 2;
+    o->norm = 0;
+    o->g_tol = 1.4901161193847656e-08;
+    o->kappa = 0.1;
+    o->roundoff = 0;
+    o->rate_test = 1;
+}
+
+void gsb_default_method(GsbMethod* m) {
+    std::memset(m, 0, sizeof(*m));
+    m->linsolve = GSB_LU;
+    m->factor_precision = GSB_F64;
+    m->refinement = GSB_NO_REFINEMENT;
+    m->refine_maxiter = 5;
+    m->refine_eta = 1.4901161193847656e-08;
+    m->globalization = GSB_BACKTRACKING;
+    m->bt_maxiter = 100;
+    m->static_alpha = 1.0;
+    m->bt_c1 = 1e-4;
+    m->bt_p = 0.5;
+    m->lm_mu0 = 1e-6;
+    m->lm_mu_min = 1e-15;
+    m->lm_mu_max = 1e12;
+    m->lm_mu_decrease = 1.0 / 3.0;
+    m->lm_mu_increase = 4.0;
+    m->lm_rho_accept = 0.0;
+    m->regularization = 0.0;
+    m->arithmetic = GSB_FUSED;
+}
+
+int gsb_solve_batch(const GsbProblem* prob, const GsbMethod* method, const GsbOptions* opt,
+                    double* X, int32_t x_layout, void* S, int32_t s_kind, const double* P,
+                    int32_t p_layout, const int64_t* order, int32_t order_base, int64_t nsys,
+                    void* stream, GsbTally* tally) {
+    g_err.clear();
+    if (!prob || !method || !opt) return set_err(GSB_ERR_ARGUMENT, "null problem, method or options");
+    if (nsys < 0) return set_err(GSB_ERR_DIMENSION, "negative batch length");
+    if (int rc = check_options(opt)) return rc;
+    if (int rc = check_method(method)) return rc;
+    int64_t np = param_count(prob);
+    if (np < 0) return set_err(GSB_ERR_ARGUMENT, "unknown family or size");
+    if (x_layout != GSB_AOS && x_layout != GSB_SOA) return set_err(GSB_ERR_ARGUMENT, "x_layout");
+    if (p_layout != GSB_AOS && p_layout != GSB_SOA) return set_err(GSB_ERR_ARGUMENT, "p_layout");
+    if (s_kind != GSB_STATUS64 && s_kind != GSB_CODES) return set_err(GSB_ERR_ARGUMENT, "s_kind");
+    if (order_base != 0 && order_base != 1) return set_err(GSB_ERR_ARGUMENT, "order_base");
+    if (tally) std::memset(tally, 0, sizeof(*tally));
+    if (nsys == 0) return 0;
+    if (!X || !S || !P) return set_err(GSB_ERR_ARGUMENT, "null X, S or P");
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    if (order) {
+        // isperm, as the reference checks on the host (src/nonlinear/batched.jl:134-136)
+        std::vector<int64_t> h(nsys);
+        if (int rc = cuda_err(cudaMemcpyAsync(h.data(), order, nsys * sizeof(int64_t),
+                                              cudaMemcpyDeviceToHost, st), "order copy"))
+            return rc;
+        if (int rc = cuda_err(cudaStreamSynchronize(st), "order copy")) return rc;
+        std::vector<char> seen(nsys, 0);
+        for (int64_t q = 0; q < nsys; ++q) {
+            int64_t v = h[q] - order_base;
+            if (v < 0 || v >= nsys || seen[v])
+                return set_err(GSB_ERR_ARGUMENT, "order is not a permutation of the batch");
+            seen[v] = 1;
+        }
+    }
+    if (method->globalization == GSB_LEVENBERG_MARQUARDT)
+        return set_err(GSB_ERR_UNSUPPORTED, "LevenbergMarquardt batch kernel not in this build");
+    if (method->linsolve != GSB_LU)
+        return set_err(GSB_ERR_UNSUPPORTED, "QRFactorization batch kernel not in this build");
+    const bool mixed = method->factor_precision == GSB_F32;
+    const bool fused = method->arithmetic == GSB_FUSED;
+    KernelEntry* ke = select_kernel(prob, fused, mixed);
+    if (!ke) return set_err(GSB_ERR_UNSUPPORTED, "no batch kernel for this family and size");
+    Workspace* ws = nullptr;
+    if (tally) {
+        if (int rc = workspace(&ws)) return rc;
+        if (int rc = cuda_err(cudaMemsetAsync(ws->tally, 0, 6 * sizeof(unsigned long long), st),
+                              "cudaMemsetAsync"))
+            return rc;
+    }
+    int dev = 0;
+    cudaGetDevice(&dev);
+    size_t smem = (size_t)kThreads * ke->row * sizeof(double);
+    if (!ke->attr_set[dev & 63]) {
+        if (int rc = cuda_err(cudaFuncSetAttribute(reinterpret_cast<const void*>(ke->fn),
+                                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   (int)smem),
+                              "cudaFuncSetAttribute"))
+            return rc;
+        ke->attr_set[dev & 63] = true;
+    }
+    Launch L{X, x_layout, S, s_kind, P, p_layout, order, order_base, nsys, prob->shared,
+             ws ? ws->tally : nullptr};
+    int64_t blocks = (nsys + kThreads - 1) / kThreads;
+    ke->fn<<<(unsigned)blocks, kThreads, smem, st>>>(*method, *opt, L);
+    if (int rc = cuda_err(cudaGetLastError(), "kernel launch")) return rc;
+    if (tally) {
+        unsigned long long h[6];
+        if (int rc = cuda_err(cudaMemcpyAsync(h, ws->tally, sizeof(h), cudaMemcpyDeviceToHost, st),
+                              "tally copy"))
+            return rc;
+        if (int rc = cuda_err(cudaStreamSynchronize(st), "tally copy")) return rc;
+        for (int c = 0; c < 6; ++c) tally->counts[c] = (int64_t)h[c];
+    }
+    return 0;
+}
+
+int gsb_batch_summary(const GsbStatus64* S, int64_t nsys, void* stream, GsbSummary* out) {
+    g_err.clear();
+    if (!out) return set_err(GSB_ERR_ARGUMENT, "null output");
+    std::memset(out, 0, sizeof(*out));
+    if (nsys == 0) {
+        out->all_converged = 1;
+        return 0;
+    }
+    if (!S) return set_err(GSB_ERR_ARGUMENT, "null statuses");
+    Workspace* ws = nullptr;
+    if (int rc = workspace(&ws)) return rc;
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    SummaryAcc h{};
+    if (int rc = cuda_err(cudaMemsetAsync(ws->acc, 0, sizeof(SummaryAcc), st), "memset")) return rc;
+    int blocks = (int)((nsys + 255) / 256);
+    blocks = blocks > 1184 ? 1184 : blocks;
+    summary_kernel<<<blocks, 256, 0, st>>>(reinterpret_cast<const unsigned char*>(S), nsys, ws->acc,
+                                           0, 0);
+    if (int rc = cuda_err(cudaMemcpyAsync(&h, ws->acc, sizeof(h), cudaMemcpyDeviceToHost, st), "copy"))
+        return rc;
+    if (int rc = cuda_err(cudaStreamSynchronize(st), "sync")) return rc;
+    double s = h.sumsq;
+    double mx;
+    std::memcpy(&mx, &h.maxbits, sizeof(double));
+    double fnorm;
+    if (h.nan_seen) {
+        fnorm = __builtin_nan("");
+    } else if (std::isfinite(s) && s >= (double)nsys * 2.2250738585072014e-308) {
+        fnorm = std::sqrt(s);
+    } else if (mx == 0.0 || !std::isfinite(mx)) {
+        fnorm = mx;
+    } else {
+        int e = std::ilogb(mx);
+        double zero = 0.0;
+        if (int rc = cuda_err(cudaMemcpyAsync(&ws->acc->sumsq, &zero, sizeof(double),
+                                              cudaMemcpyHostToDevice, st), "copy"))
+            return rc;
+        summary_kernel<<<blocks, 256, 0, st>>>(reinterpret_cast<const unsigned char*>(S), nsys,
+                                               ws->acc, e, 1);
+        double s2 = 0;
+        if (int rc = cuda_err(cudaMemcpyAsync(&s2, &ws->acc->sumsq, sizeof(double),
+                                              cudaMemcpyDeviceToHost, st), "copy"))
+            return rc;
+        if (int rc = cuda_err(cudaStreamSynchronize(st), "sync")) return rc;
+        fnorm = std::ldexp(std::sqrt(s2), e);
+    }
+    out->fnorm = fnorm;
+    out->failure_count = (int64_t)h.failures;
+    out->all_converged = h.failures == 0;
+    out->max_iterations = h.max_iterations;
+    out->total_iterations = (int64_t)h.total_iterations;
+    return 0;
+}
+
+int gsb_synchronize(void* stream) {
+    return cuda_err(cudaStreamSynchronize(reinterpret_cast<cudaStream_t>(stream)),
+                    "cudaStreamSynchronize");
+}
+
+}  // extern "C"

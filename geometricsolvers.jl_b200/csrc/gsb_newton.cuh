@@ -1,0 +1,758 @@
+// The per-system Newton solve of the batch: one CUDA thread runs GeometricSolvers.jl's R1 loop
+// `solve!!` (src/nonlinear/solver.jl:277-378) for its system, with the iterate, the residual,
+// the Jacobian, its pivoted factor and the direction in registers (every array index is a
+// compile-time constant after unrolling; a pivot row is selected by predicated moves).
+//
+// Methods: Newton with LUFactorization{TF} (TF = Float64, or Float32 with Refinement and the
+// promotion to Float64 of src/nonlinear/newton.jl:1604-1720), globalization Static or
+// Backtracking. Status fields, codes and every stopping test follow the reference.
+#pragma once
+
+#include "../../include/gsb.h"
+#include "gsb_families.cuh"
+#include "gsb_numerics.cuh"
+
+namespace gsb {
+
+struct StepInfo {
+    int code;
+    double fnorm, stepnorm;
+    int failures;
+    bool promoted, limited, shortened;
+};
+
+struct DevStatus {
+    int code, iterations;
+    double fnorm, stepnorm;
+    int step_failures;
+    bool promoted, stationary;
+    double rate;
+    bool contracted;
+};
+
+struct DevState {
+    double merit, fnorm, gradratio, jnorm;
+    bool promoted;
+    int slow_steps;
+};
+
+// record(status, info), src/base/status.jl:245-262.
+__device__ __forceinline__ void record(DevStatus& s, const StepInfo& i) {
+    s.rate = s.stepnorm > 0.0 ? __ddiv_rn(i.stepnorm, s.stepnorm) : kNaN;
+    s.code = i.code;
+    s.iterations += 1;
+    s.fnorm = i.fnorm;
+    s.stepnorm = i.stepnorm;
+    s.step_failures += i.failures;
+    s.promoted = s.promoted || i.promoted;
+}
+
+// Exchange x and y where r == p, as two predicated selects. Written in PTX so that the front
+// end cannot turn a row exchange over unrolled rows into an indexed access, which would move the
+// whole register matrix to local memory. Both selects write PTX temporaries before either
+// output is written, so an output that shares a register with an input cannot corrupt it.
+__device__ __forceinline__ void cswap(int r, int p, double& x, double& y) {
+    double nx, ny;
+    asm("{\n\t.reg .pred q;\n\t.reg .f64 t0, t1;\n\tsetp.eq.s32 q, %2, %3;\n\t"
+        "selp.f64 t0, %5, %4, q;\n\tselp.f64 t1, %4, %5, q;\n\tmov.f64 %0, t0;\n\t"
+        "mov.f64 %1, t1;\n\t}"
+        : "=d"(nx), "=d"(ny)
+        : "r"(r), "r"(p), "d"(x), "d"(y));
+    x = nx;
+    y = ny;
+}
+__device__ __forceinline__ void cswap(int r, int p, float& x, float& y) {
+    float nx, ny;
+    asm("{\n\t.reg .pred q;\n\t.reg .f32 t0, t1;\n\tsetp.eq.s32 q, %2, %3;\n\t"
+        "selp.f32 t0, %5, %4, q;\n\tselp.f32 t1, %4, %5, q;\n\tmov.f32 %0, t0;\n\t"
+        "mov.f32 %1, t1;\n\t}"
+        : "=f"(nx), "=f"(ny)
+        : "r"(r), "r"(p), "f"(x), "f"(y));
+    x = nx;
+    y = ny;
+}
+
+// The pivoted LU of src/linear/static/lu.jl:24-64 on a register matrix, with the scaling of
+// factor_matrix (src/linear/factors.jl:802-811): TF = T divides by 2^e only for e < 0; another
+// TF divides for every e != 0, in T, then rounds to TF.
+template <bool F, int N, class TF> struct LUFactor {
+    TF a[N * N];
+    int ipiv[N];
+    int info;
+    int e;
+
+    template <class Fam, class JS>
+    __device__ __forceinline__ void factor(const Fam& fam, const JS& js) {
+        // J into the factor's registers, then J / 2^e in place (factor_matrix)
+        constexpr bool same = sizeof(TF) == sizeof(double);
+        if constexpr (same) {
+#pragma unroll
+            for (int k = 0; k < N; ++k)
+#pragma unroll
+                for (int i = 0; i < N; ++i) a[i + k * N] = fam.J(js, i, k);
+            e = matrix_exponent<N * N>(a);
+            if (e < 0) {
+#pragma unroll
+                for (int q = 0; q < N * N; ++q) a[q] = scale2_in(a[q], -e);  // -e in [1, 1023]
+            } else {
+                e = 0;
+            }
+        } else {
+            unsigned long long mb = 0;
+#pragma unroll
+            for (int k = 0; k < N; ++k)
+#pragma unroll
+                for (int i = 0; i < N; ++i) {
+                    unsigned long long b = FBits<double>::bits(fam.J(js, i, k)) & ~FBits<double>::sign_mask;
+                    mb = b > mb ? b : mb;
+                }
+            double mm = FBits<double>::from(mb);
+            e = (isfin(mm) && mm != 0.0) ? max(-1023, min(1023, jexponent(mm))) : 0;
+#pragma unroll
+            for (int k = 0; k < N; ++k)
+#pragma unroll
+                for (int i = 0; i < N; ++i) {
+                    double v = fam.J(js, i, k);
+                    a[i + k * N] = TF(e == 0 ? v : scale2_in(v, -e));  // -e in [-1023, 1023]
+                }
+        }
+        info = 0;
+#pragma unroll
+        for (int k = 0; k < N; ++k) {
+            int p = k;
+            TF amax = fabs(a[k + k * N]);
+#pragma unroll
+            for (int i = k + 1; i < N; ++i) {
+                TF v = fabs(a[i + k * N]);
+                if (v > amax) {
+                    amax = v;
+                    p = i;
+                }
+            }
+            ipiv[k] = p;
+            if (p != k) {
+#pragma unroll
+                for (int i = k + 1; i < N; ++i)
+#pragma unroll
+                    for (int j = 0; j < N; ++j) cswap(i, p, a[k + j * N], a[i + j * N]);
+            }
+            TF akk = a[k + k * N];
+            if (akk == TF(0)) {
+                if (info == 0) info = k + 1;
+            } else {
+#pragma unroll
+                for (int i = k + 1; i < N; ++i) a[i + k * N] = a[i + k * N] / akk;
+#pragma unroll
+                for (int j = k + 1; j < N; ++j)
+#pragma unroll
+                    for (int i = k + 1; i < N; ++i)
+                        a[i + j * N] = Arith<F>::msub(a[i + k * N], a[k + j * N], a[i + j * N]);
+            }
+        }
+    }
+
+    // lu.jl:67-92.
+    __device__ __forceinline__ void backsolve(TF (&x)[N]) const {
+#pragma unroll
+        for (int k = 0; k < N; ++k) {
+            int p = ipiv[k];
+            if (p != k) {
+#pragma unroll
+                for (int i = k + 1; i < N; ++i) cswap(i, p, x[k], x[i]);
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < N; ++k) {
+            TF xk = x[k];
+#pragma unroll
+            for (int i = k + 1; i < N; ++i) x[i] = Arith<F>::msub(a[i + k * N], xk, x[i]);
+        }
+#pragma unroll
+        for (int k = N - 1; k >= 0; --k) {
+            TF xk = x[k] / a[k + k * N];
+            x[k] = xk;
+#pragma unroll
+            for (int i = 0; i < k; ++i) x[i] = Arith<F>::msub(a[i + k * N], xk, x[i]);
+        }
+    }
+
+    // ldiv!!: same type (factors.jl:931-936) or mixed type (factors.jl:943-949).
+    __device__ __forceinline__ void ldiv(const double (&r)[N], double (&d)[N]) const {
+        if constexpr (sizeof(TF) == sizeof(double)) {
+            int k = rhs_exponent<N>(r, e);
+            TF x[N];
+#pragma unroll
+            for (int i = 0; i < N; ++i) x[i] = k == 0 ? r[i] : scale2_in(r[i], -k);  // -k in [-6, 1023]
+            backsolve(x);
+            int e2 = k - e;
+#pragma unroll
+            for (int i = 0; i < N; ++i) d[i] = e2 == 0 ? double(x[i]) : scale2_in(double(x[i]), e2);  // e2 = k - e in [0, 1029]
+        } else {
+            double s = fabs(r[0]);
+#pragma unroll
+            for (int i = 1; i < N; ++i) s = jmax(s, fabs(r[i]));
+            if (s == 0.0) {
+#pragma unroll
+                for (int i = 0; i < N; ++i) d[i] = 0.0;
+                return;
+            }
+            TF x[N];
+#pragma unroll
+            for (int i = 0; i < N; ++i) x[i] = TF(__ddiv_rn(r[i], s));
+            backsolve(x);
+            int ex = 0;
+            double frac = isfin(s) ? frexp(s, &ex) : s;
+            if (!isfin(s)) ex = 0;
+#pragma unroll
+            for (int i = 0; i < N; ++i) d[i] = __dmul_rn(double(x[i]), frac);
+            const int E = ex - e;
+            if (E >= -1074 && E <= 2046) {
+#pragma unroll
+                for (int i = 0; i < N; ++i) d[i] = scale2_in(d[i], E);
+            } else {
+#pragma unroll
+                for (int i = 0; i < N; ++i) d[i] = ldexp2_slow(d[i], E);
+            }
+        }
+    }
+};
+
+template <class Fam, bool F, bool Mixed> struct Solver {
+    static constexpr int N = Fam::N, M = Fam::M;
+    using JS = typename Fam::JState;
+    using A = Arith<F>;
+    const Fam& fam;
+    const GsbMethod& m;
+    const GsbOptions& o;
+    double* stash;  // this thread's 2N doubles of shared memory, or nullptr
+
+    __device__ Solver(const Fam& f, const GsbMethod& mm, const GsbOptions& oo, double* st)
+        : fam(f), m(mm), o(oo), stash(st) {}
+
+    // While a factor holds the registers, the iterate and the residual wait in shared memory:
+    // a volatile store and a volatile load, so that their register copies are free meanwhile.
+    __device__ __forceinline__ void park(double (&x)[N], double (&Fx)[M]) const {
+        if (stash == nullptr) return;
+        volatile double* v = stash;
+#pragma unroll
+        for (int i = 0; i < N; ++i) v[i] = x[i];
+#pragma unroll
+        for (int i = 0; i < M; ++i) v[N + i] = Fx[i];
+    }
+    __device__ __forceinline__ void unpark_x(double (&x)[N]) const {
+        if (stash == nullptr) return;
+        volatile double* v = stash;
+#pragma unroll
+        for (int i = 0; i < N; ++i) x[i] = v[i];
+    }
+    __device__ __forceinline__ void unpark_F(double (&Fx)[M]) const {
+        if (stash == nullptr) return;
+        volatile double* v = stash;
+#pragma unroll
+        for (int i = 0; i < M; ++i) Fx[i] = v[N + i];
+    }
+
+    __device__ __forceinline__ bool has_merit() const { return m.globalization == GSB_BACKTRACKING; }
+
+    // J v as a left fold over the columns (the SMatrix product of the held Jacobian).
+    __device__ __forceinline__ void jmul(const JS& js, const double (&v)[N], double (&out)[M]) const {
+#pragma unroll
+        for (int i = 0; i < M; ++i) {
+            double s = A::mul(fam.J(js, i, 0), v[0]);
+#pragma unroll
+            for (int k = 1; k < N; ++k) s = A::madd(fam.J(js, i, k), v[k], s);
+            out[i] = s;
+        }
+    }
+
+    // grad_ratio_and_norm, src/nonlinear/newton.jl:1287-1298.
+    __device__ void grad_ratio_and_norm(const JS& js, const double (&Fx)[M], double fnorm,
+                                        double& gr, double& jnorm) const {
+        double s = A::mul(fam.J(js, 0, 0), fam.J(js, 0, 0));
+        double m0 = 0.0;
+#pragma unroll
+        for (int k = 0; k < N; ++k)
+#pragma unroll
+            for (int i = 0; i < M; ++i) {
+                if (i == 0 && k == 0) continue;
+                double v = fam.J(js, i, k);
+                s = A::madd(v, v, s);
+            }
+        const double tiny = double(M * N) * kFloatmin;
+        if (isfin(s) && s >= tiny) {
+            jnorm = sqrt(s);
+        } else {
+            // scaled fallback of rnorm over the M*N entries
+            double mx = 0.0;
+#pragma unroll
+            for (int k = 0; k < N; ++k)
+#pragma unroll
+                for (int i = 0; i < M; ++i) mx = jmax(mx, jmax(fabs(fam.J(js, i, k)), 0.0));
+            if (mx == 0.0 || !isfin(mx)) {
+                jnorm = mx;
+            } else {
+                int e = jexponent(mx);
+                double acc = 0.0;
+                bool first = true;
+#pragma unroll
+                for (int k = 0; k < N; ++k)
+#pragma unroll
+                    for (int i = 0; i < M; ++i) {
+                        double u = scale2_in(fam.J(js, i, k), -e);
+                        acc = first ? A::mul(u, u) : A::madd(u, u, acc);
+                        first = false;
+                    }
+                jnorm = scale2_in(sqrt(acc), e);
+            }
+        }
+        (void)m0;
+        if (jnorm == 0.0 || fnorm == 0.0) {
+            gr = 0.0;
+            return;
+        }
+        double g[N];
+#pragma unroll
+        for (int j = 0; j < N; ++j) {
+            double t = A::mul(fam.J(js, 0, j), Fx[0]);
+#pragma unroll
+            for (int i = 1; i < M; ++i) t = A::madd(fam.J(js, i, j), Fx[i], t);
+            g[j] = t;
+        }
+        double gnorm = rnorm<F, N>(g);
+        if (isfin(gnorm) || !(isfin(jnorm) && isfin(fnorm))) {
+            gr = __ddiv_rn(__ddiv_rn(gnorm, jnorm), fnorm);
+            return;
+        }
+        int e = jexponent(fnorm);
+        double sc = ldexp(1.0, -e);
+#pragma unroll
+        for (int j = 0; j < N; ++j) {
+            double t = A::mul(fam.J(js, 0, j), __dmul_rn(Fx[0], sc));
+#pragma unroll
+            for (int i = 1; i < M; ++i) t = A::madd(fam.J(js, i, j), __dmul_rn(Fx[i], sc), t);
+            g[j] = t;
+        }
+        gr = __ddiv_rn(__ddiv_rn(rnorm<F, N>(g), jnorm), ldexp(fnorm, -e));
+    }
+
+    // residual_norm, src/nonlinear/newton.jl:1274-1278.
+    __device__ __forceinline__ double residual_norm(const DevState& st, const double (&Fx)[M]) const {
+        if (has_merit()) {
+            if (isfin(st.merit) && st.merit >= double(M) * kFloatmin) return sqrt(st.merit);
+            return rnorm<F, M>(Fx);
+        }
+        return isnan(st.fnorm) ? rnorm<F, M>(Fx) : st.fnorm;
+    }
+
+    // The merit of the trial x + a d: the trial iterate, its residual and norm2.
+    __device__ __forceinline__ double trial(const double (&x)[N], const double (&d)[N], double a,
+                                            double (&xt)[N], double (&Ft)[M]) const {
+#pragma unroll
+        for (int i = 0; i < N; ++i) xt[i] = A::madd(a, d[i], x[i]);
+        fam.F(xt, Ft);
+        return norm2<F, M>(Ft);
+    }
+
+    // φ′(0) = 2 <F(x), J(x) d> (src/globalization/linefunction.jl:47-52).
+    __device__ __forceinline__ double slope0(const double (&x)[N], const double (&d)[N]) const {
+        double x0[N], F0[M], Jv[M];
+#pragma unroll
+        for (int i = 0; i < N; ++i) x0[i] = A::madd(0.0, d[i], x[i]);
+        fam.F(x0, F0);
+        fam.jvp(x0, d, Jv);
+        double s = A::mul(F0[0], Jv[0]);
+#pragma unroll
+        for (int i = 1; i < M; ++i) s = A::madd(F0[i], Jv[i], s);
+        return 2.0 * s;
+    }
+
+    // globalize!! for Static (src/globalization/linefunction.jl:114-131) and globalize_merit!!
+    // with the Backtracking search (linefunction.jl:159-199, linesearch.jl:154-171,
+    // backtracking.jl:62-132).
+    __device__ void globalize(double (&x)[N], double (&Fx)[M], const double (&d)[N], bool exact,
+                              double& merit, StepInfo& info) const {
+        if (m.globalization == GSB_STATIC) {
+            double s = m.static_alpha;
+            double dn = rnorm<F, N>(d);
+            double stepnorm = __dmul_rn(fabs(s), dn);
+            if (!isfin(stepnorm)) {
+                info = {NONFINITE, rnorm<F, M>(Fx), stepnorm, 0, false, false, false};
+                return;
+            }
+            double xp[N], Fp[M];
+            double fn = rnorm_from<F, M>(Fp, trial(x, d, s, xp, Fp));
+            if (!isfin(fn)) {
+                info = {NONFINITE, rnorm<F, M>(Fx), stepnorm, 0, false, false, false};
+                return;
+            }
+#pragma unroll
+            for (int i = 0; i < N; ++i) x[i] = xp[i];
+#pragma unroll
+            for (int i = 0; i < M; ++i) Fx[i] = Fp[i];
+            info = {SUCCESS, fn, stepnorm, 0, false, false, false};
+            return;
+        }
+        const double phi0 = merit;
+        double dn = rnorm<F, N>(d);
+        if (!isfin(dn)) {
+            info = {NONFINITE, rnorm<F, M>(Fx), dn, 0, false, false, false};
+            return;
+        }
+        // linesearch entry: trial step 1, the anchor slope, τ and the step floor
+        double alpha = 1.0;
+        double d0 = exact ? -2.0 * phi0 : slope0(x, d);
+        int code;
+        double aa = alpha, pa = kNaN;
+        double xt[N], Ft[M];
+        if (!(isfin(phi0) && isfin(d0) && d0 < 0.0)) {
+            code = (isfin(phi0) && isfin(d0)) ? (d0 > 0.0 ? LINESEARCH_FAILED : STALLED) : NONFINITE;
+        } else {
+            double tau = jmax(__dmul_rn(4.0 * kEps, fabs(phi0)), 4.0 * 4.9406564584124654e-324);
+            double amin = jmax(__ddiv_rn(tau, fabs(d0)), kFloatmin);
+            alpha = jmin(jmax(alpha, amin), kInf);
+            double ap = kNaN, pp = kNaN;
+            int frozen = 0, trips = 0;
+            code = LINESEARCH_FAILED;
+            bool done = false;
+            const double c1 = m.bt_c1, p = m.bt_p;
+            while (!done && trips < m.bt_maxiter) {
+                ++trips;
+                aa = alpha;
+                pa = trial(x, d, alpha, xt, Ft);
+                frozen = (pa == phi0 && alpha <= kSqrtEps) ? frozen + 1 : 0;
+                double demand = __dmul_rn(__dmul_rn(c1, alpha), d0);
+                if (__dsub_rn(pa, phi0) <= jmin(0.0, __dadd_rn(demand, tau))) {
+                    // classify
+                    if (isfin(pa) && __dsub_rn(pa, phi0) < -tau) code = SUCCESS;
+                    else code = fabs(__dsub_rn(pa, phi0)) <= tau ? STALLED : LINESEARCH_FAILED;
+                    done = true;
+                } else if (frozen >= 2) {
+                    code = STALLED;
+                    done = true;
+                } else if (alpha <= amin) {
+                    code = fabs(__dsub_rn(pa, phi0)) <= tau ? STALLED : LINESEARCH_FAILED;
+                    done = true;
+                } else {
+                    double an;
+                    if (isfin(pa)) {
+                        // backtrack_step, backtracking.jl:62-82
+                        an = kNaN;
+                        double s = fabs(d0);
+                        double r1 = __dadd_rn(__ddiv_rn(__dsub_rn(pa, phi0), s), alpha);
+                        if (!(ap > 0.0)) {
+                            if (r1 > 0.0) an = __ddiv_rn(__dmul_rn(alpha, alpha), __dmul_rn(2.0, r1));
+                        } else if (isfin(pp) && alpha != ap) {
+                            double q1 = __ddiv_rn(r1, __dmul_rn(alpha, alpha));
+                            double q2 = __ddiv_rn(__dadd_rn(__ddiv_rn(__dsub_rn(pp, phi0), s), ap),
+                                                  __dmul_rn(ap, ap));
+                            double da = __dsub_rn(alpha, ap);
+                            double Aq = __ddiv_rn(__dsub_rn(q1, q2), da);
+                            double Bq = __ddiv_rn(__dsub_rn(__dmul_rn(alpha, q2), __dmul_rn(ap, q1)), da);
+                            double disc = __dadd_rn(__dmul_rn(Bq, Bq), __dmul_rn(3.0, Aq));
+                            if (disc >= 0.0)
+                                an = Bq > 0.0 ? __ddiv_rn(1.0, __dadd_rn(Bq, sqrt(disc)))
+                                              : __ddiv_rn(__dadd_rn(-Bq, sqrt(disc)), __dmul_rn(3.0, Aq));
+                        }
+                        if (!(isfin(an) && an > 0.0)) an = __dmul_rn(p, alpha);
+                        an = jmin(jmax(an, __dmul_rn(0.1, alpha)), __dmul_rn(p, alpha));
+                    } else {
+                        an = jmin(__dmul_rn(0.1, alpha), __dmul_rn(sqrt(alpha), sqrt(amin)));
+                    }
+                    ap = alpha;
+                    pp = pa;
+                    alpha = jmax(an, amin);
+                }
+            }
+        }
+        if (code == SUCCESS) {
+#pragma unroll
+            for (int i = 0; i < N; ++i) x[i] = xt[i];
+#pragma unroll
+            for (int i = 0; i < M; ++i) Fx[i] = Ft[i];
+            info = {SUCCESS, sqrt(pa), __dmul_rn(aa, dn), 0, false, false, aa < 1.0};
+            merit = pa;
+        } else if (code == LINESEARCH_FAILED) {
+            if (isfin(pa) && pa < phi0) {
+#pragma unroll
+                for (int i = 0; i < N; ++i) x[i] = xt[i];
+#pragma unroll
+                for (int i = 0; i < M; ++i) Fx[i] = Ft[i];
+                info = {LINESEARCH_FAILED, sqrt(pa), __dmul_rn(aa, dn), 1, false, false, aa < 1.0};
+                merit = pa;
+            } else {
+                info = {LINESEARCH_FAILED, rnorm<F, M>(Fx), 0.0, 1, false, false, false};
+            }
+        } else if (code == STALLED) {
+            info = {STALLED, rnorm<F, M>(Fx), 0.0, 0, false, false, false};
+        } else {
+            info = {NONFINITE, rnorm<F, M>(Fx), 0.0, 0, false, false, false};
+        }
+    }
+
+    // refine_passes!! with the held Jacobian, src/nonlinear/refinement.jl:211-244; returns
+    // `failed`.
+    template <class Fac>
+    __device__ bool refine(double (&d)[N], const Fac& fac, const JS& js, const double (&Fx)[M]) const {
+        double fnorm = rnorm<F, M>(Fx);
+        if (fnorm == 0.0) return false;
+        if (!isfin(fnorm)) return true;
+        double eta = jmax(m.refine_eta, kSqrtEps);
+        double thr = __dmul_rn(eta, fnorm);
+        double Jv[N], r[N];
+        jmul(js, d, Jv);
+#pragma unroll
+        for (int i = 0; i < N; ++i) r[i] = __dadd_rn(-Fx[i], -Jv[i]);
+        double rprev = rnorm<F, N>(r);
+        if (!isfin(rprev)) return true;
+        if (rprev <= thr) return false;
+        for (int it = 1; it <= m.refine_maxiter; ++it) {
+            double dd[N], dc[N];
+            fac.ldiv(r, dd);
+#pragma unroll
+            for (int i = 0; i < N; ++i) dc[i] = __dadd_rn(d[i], dd[i]);
+            jmul(js, dc, Jv);
+#pragma unroll
+            for (int i = 0; i < N; ++i) r[i] = __dadd_rn(-Fx[i], -Jv[i]);
+            double rc = rnorm<F, N>(r);
+            if (!(rc < rprev)) return true;
+#pragma unroll
+            for (int i = 0; i < N; ++i) d[i] = dc[i];
+            rprev = rc;
+            if (rc <= thr) return false;
+        }
+        return true;
+    }
+
+    // The plain step (TF = T), src/nonlinear/newton.jl:1679-1688.
+    __device__ void step_plain(DevState& st, double (&x)[N], double (&Fx)[M], StepInfo& info) const {
+        double fnorm = residual_norm(st, Fx);
+        JS js;
+        fam.jacobian(x, js);
+        double gr, jn;
+        grad_ratio_and_norm(js, Fx, fnorm, gr, jn);
+        double merit = st.merit;
+        const bool ref = m.refinement == GSB_REFINEMENT;
+        {
+            park(x, Fx);
+            LUFactor<F, N, double> fac;
+            fac.factor(fam, js);
+            if (fac.info > 0) {
+                unpark_x(x);
+                unpark_F(Fx);
+                info = {SINGULAR, rnorm<F, M>(Fx), 0.0, 0, false, false, false};
+            } else {
+                double d[N];
+                unpark_F(Fx);
+                fac.ldiv(Fx, d);
+#pragma unroll
+                for (int i = 0; i < N; ++i) d[i] = -d[i];
+                if (ref) refine(d, fac, js, Fx);
+                unpark_x(x);
+                globalize(x, Fx, d, !ref, merit, info);
+            }
+        }
+        st.gradratio = gr;
+        st.jnorm = jn;
+        st.merit = merit;
+        st.fnorm = info.fnorm;
+    }
+
+    // The mixed-precision step (TF = Float32), src/nonlinear/newton.jl:1692-1720 with
+    // mixed_newton!! :1604-1666, promote_factor!! :1332-1339, linear_residual_ratio :1422-1430
+    // and read_mixed_stall :1437-1451.
+    __device__ void step_mixed(DevState& st, double (&x)[N], double (&Fx)[M], StepInfo& info) const {
+        double fnorm_old = residual_norm(st, Fx);
+        const bool was_promoted = st.promoted;
+        JS js;
+        fam.jacobian(x, js);
+        double gr, jn;
+        grad_ratio_and_norm(js, Fx, fnorm_old, gr, jn);
+        st.gradratio = gr;
+        st.jnorm = jn;
+        const bool ref = m.refinement == GSB_REFINEMENT;
+        double d[N];
+        bool ok = true;
+        int failures = 0;
+        double lin_rel = 0.0;
+        bool md_promoted = was_promoted;
+        bool fallback = was_promoted;
+        if (!was_promoted) {
+            LUFactor<F, N, float> fac;
+            fac.factor(fam, js);
+            bool ref_failed;
+            if (fac.info > 0) {
+                ref_failed = true;
+            } else {
+                fac.ldiv(Fx, d);
+#pragma unroll
+                for (int i = 0; i < N; ++i) d[i] = -d[i];
+                ref_failed = ref ? refine(d, fac, js, Fx) : false;
+            }
+            if (ref_failed || fac.info > 0) {
+                failures += 1;
+                md_promoted = true;
+                fallback = true;
+            } else if (!Fam::lsq) {
+                if (fnorm_old == 0.0 || !isfin(fnorm_old)) {
+                    lin_rel = 0.0;
+                } else {
+                    double Jd[N], lin[N];
+                    jmul(js, d, Jd);
+#pragma unroll
+                    for (int i = 0; i < N; ++i) lin[i] = __dadd_rn(Fx[i], Jd[i]);
+                    lin_rel = __ddiv_rn(rnorm<F, N>(lin), fnorm_old);
+                }
+            }
+        }
+        if (fallback) {
+            // the factorisation in the working precision: at every step once promoted (with the
+            // refinement passes), and as the promotion of a failed Float32 step (without them)
+            LUFactor<F, N, double> ft;
+            ft.factor(fam, js);
+            if (ft.info > 0) {
+                ok = false;
+            } else {
+                ft.ldiv(Fx, d);
+#pragma unroll
+                for (int i = 0; i < N; ++i) d[i] = -d[i];
+                if (was_promoted && ref) refine(d, ft, js, Fx);
+            }
+        }
+        if (!ok) {
+            st.promoted = md_promoted;
+            info = {SINGULAR, rnorm<F, M>(Fx), 0.0, failures, md_promoted, false, false};
+            return;
+        }
+        const bool promoted_step = md_promoted && !was_promoted;
+        const bool exact_step = md_promoted && !Fam::lsq;
+        double merit = st.merit;
+        globalize(x, Fx, d, exact_step, merit, info);
+        info.failures += failures;
+        if (promoted_step) {
+            info.promoted = true;
+            st.promoted = true;
+            st.slow_steps = 0;
+        } else if (!was_promoted) {
+            const double eta_lin = 1e-4;
+            if (info.fnorm > __dmul_rn(0.5, fnorm_old) && lin_rel > eta_lin) {
+                int slow = st.slow_steps + 1;
+                if (slow >= 2) {
+                    st.promoted = true;
+                    st.slow_steps = 0;
+                    info.failures += 1;
+                    info.promoted = true;
+                } else {
+                    st.promoted = false;
+                    st.slow_steps = slow;
+                }
+            } else {
+                st.promoted = false;
+                st.slow_steps = 0;
+            }
+        }
+        st.merit = merit;
+        st.fnorm = info.fnorm;
+    }
+
+    __device__ __forceinline__ bool residual_converged(const DevStatus& s, double ftest,
+                                                       double ftest0) const {
+        if (!(s.iterations >= o.min_iterations)) return false;
+        return ftest <= jmax(o.f_abstol, __dmul_rn(o.f_reltol, ftest0));
+    }
+
+    // solve!!, src/nonlinear/solver.jl:277-378. Returns the status; `gr` is the gradratio of
+    // the last factorisation (newton_finish!!, src/nonlinear/newton.jl:1165-1184).
+    __device__ DevStatus solve(double (&x)[N], double& gr_out) const {
+        double Fx[M];
+        fam.F(x, Fx);
+        double n2 = norm2<F, M>(Fx);
+        double fnorm0 = rnorm_from<F, M>(Fx, n2);
+        DevState st;
+        st.merit = has_merit() ? n2 : kNaN;
+        st.fnorm = fnorm0;
+        st.gradratio = kNaN;
+        st.jnorm = 0.0;
+        st.promoted = false;
+        st.slow_steps = 0;
+        DevStatus s;
+        s.code = SUCCESS;
+        s.iterations = 0;
+        s.fnorm = fnorm0;
+        s.stepnorm = 0.0;
+        s.step_failures = 0;
+        s.promoted = false;
+        s.stationary = false;
+        s.rate = kNaN;
+        s.contracted = false;
+        gr_out = kNaN;
+        if (!isfin(fnorm0)) {
+            s.code = NONFINITE;
+            return s;
+        }
+        const double ftest0 = o.norm == 1 ? rmaxnorm<M>(Fx) : fnorm0;
+        if (residual_converged(s, ftest0, ftest0)) return s;
+        if (o.max_iterations == 0) {
+            s.code = MAXITERS;
+            return s;
+        }
+        int stalls = 0;
+        while (true) {
+            const double rate_k = s.rate;
+            StepInfo info;
+            if (Mixed) step_mixed(st, x, Fx, info);
+            else step_plain(st, x, Fx, info);
+            record(s, info);
+            gr_out = st.gradratio;
+            if (info.code == SINGULAR || info.code == NONFINITE || info.code == MAXITERS) return s;
+            if (info.code == LINESEARCH_FAILED && info.stepnorm == 0.0) return s;
+            double ft = o.norm == 1 ? rmaxnorm<M>(Fx) : s.fnorm;
+            if (residual_converged(s, ft, ftest0)) {
+                s.code = SUCCESS;
+                s.stationary = false;
+                s.contracted = false;
+                return s;
+            }
+            const bool steptested = !(info.code == STALLED || info.limited);
+            const double xnorm = steptested ? rnorm<F, N>(x) : kNaN;
+            bool contracted = false;
+            if (!info.shortened && o.rate_test && s.iterations >= o.min_iterations) {
+                double th = jmax(s.rate, rate_k);
+                if (s.stepnorm > 0.0 && th < 1.0)
+                    contracted = __dmul_rn(__ddiv_rn(th, __dsub_rn(1.0, th)), s.stepnorm) <=
+                                 __dmul_rn(o.kappa, jmax(o.x_abstol, __dmul_rn(o.x_reltol, xnorm)));
+            }
+            bool stepc = false;
+            if (steptested && s.iterations >= o.min_iterations) {
+                stepc = s.iterations > 0 && s.stepnorm > 0.0 &&
+                        s.stepnorm <= jmax(o.x_abstol, __dmul_rn(o.x_reltol, xnorm));
+                stepc = stepc || (info.code == SUCCESS && info.stepnorm == 0.0);
+                stepc = stepc || (o.roundoff && s.rate >= 1.0 && rate_k < 1.0);
+            }
+            if (contracted || stepc) {
+                s.code = contracted ? SUCCESS : STALLED;
+                s.stationary = false;
+                s.contracted = contracted;
+                return s;
+            }
+            if (info.code == STALLED) {
+                stalls += 1;
+                if (stalls >= o.max_stalls) {
+                    s.code = STALLED;
+                    s.stationary = false;
+                    s.contracted = false;
+                    return s;
+                }
+            } else {
+                stalls = 0;
+            }
+            if (s.iterations >= o.max_iterations) {
+                s.code = MAXITERS;
+                s.stationary = false;
+                s.contracted = false;
+                return s;
+            }
+        }
+    }
+};
+
+}  // namespace gsb

@@ -33,6 +33,12 @@ extern "C" {
 
 #define GSB_ABI_VERSION 1
 
+#if defined(__GNUC__)
+#define GSB_API __attribute__((visibility("default")))
+#else
+#define GSB_API
+#endif
+
 /* ReturnCode, src/base/returncodes.jl:14 (UInt8, values 0..5 in this order). */
 typedef enum {
     GSB_SUCCESS = 0,
@@ -124,6 +130,13 @@ typedef struct {
 typedef enum { GSB_LU = 0, GSB_QR = 1 } GsbLinsolve;
 typedef enum { GSB_F64 = 0, GSB_F32 = 1 } GsbPrecision;
 typedef enum { GSB_NO_REFINEMENT = 0, GSB_REFINEMENT = 1 } GsbRefinementKind;
+/* The rounding of the linear algebra (factorisation, solves, norms, products with the Jacobian).
+ * GSB_FUSED contracts each product-and-sum into one fused multiply-add (the fast default);
+ * GSB_UNFUSED rounds every product and every sum on its own, as Julia evaluates `a * b + c`, so
+ * that a batch reproduces a CPU restatement of the reference bit for bit. Residual families fix
+ * their own operation order and are the same under both. */
+typedef enum { GSB_FUSED = 0, GSB_UNFUSED = 1 } GsbArithmetic;
+
 typedef enum {
     GSB_STATIC = 0,
     GSB_BACKTRACKING = 1,
@@ -138,7 +151,7 @@ typedef enum {
  *                                  LevenbergMarquardt(mu0, mu_min, mu_max, mu_decrease,
  *                                                     mu_increase, rho_accept; scaling = :none)
  * regularization must be 0 (the default); reuse, DogLeg and the matrix-free methods are not
- * part of this ABI.
+ * part of this ABI. `arithmetic` has no counterpart in the reference (see GsbArithmetic).
  */
 typedef struct {
     int32_t linsolve;         /* GsbLinsolve */
@@ -158,6 +171,8 @@ typedef struct {
     double lm_mu_increase;
     double lm_rho_accept;
     double regularization;
+    int32_t arithmetic;       /* GsbArithmetic */
+    int32_t pad_;
 } GsbMethod;
 
 /* The six counts of the count form, src/nonlinear/batched.jl:197-199, by GsbReturnCode. */
@@ -187,23 +202,23 @@ typedef enum {
 } GsbStatusKind;
 
 /* ABI version and the sm_100a device code of this build (1 when compiled for sm_100a). */
-int gsb_abi_version(void);
+GSB_API int gsb_abi_version(void);
 
 /* The last CUDA or argument error message of this thread, or "". */
-const char* gsb_last_error(void);
+GSB_API const char* gsb_last_error(void);
 
 /* Number of parameters per system of `prob` (n*n+n for GSB_FAMILY_CUBIC_AFFINE, ...), or a
  * negative GsbError for an unknown family or size. */
-int64_t gsb_param_count(const GsbProblem* prob);
+GSB_API int64_t gsb_param_count(const GsbProblem* prob);
 
 /* Options(Float64) defaults, src/base/options.jl:207-236. */
-void gsb_default_options(GsbOptions* opt);
+GSB_API void gsb_default_options(GsbOptions* opt);
 
 /* Newton(; linsolve = LUFactorization(), globalization = Backtracking()) with the reference's
  * defaults for every field (Backtracking c1 = 1e-4, p = 0.5, maxiter = 100; Static alpha = 1;
  * Refinement eta = sqrt(eps), maxiter = 5; LevenbergMarquardt mu0 = 1e-6, mu_min = 1e-15,
  * mu_max = 1e12, mu_decrease = 1/3, mu_increase = 4, rho_accept = 0). */
-void gsb_default_method(GsbMethod* method);
+GSB_API void gsb_default_method(GsbMethod* method);
 
 /*
  * Solve every system in place: X[idx] is the start of system idx and becomes its final iterate;
@@ -215,17 +230,17 @@ void gsb_default_method(GsbMethod* method);
  * counts, which synchronises `stream`. An empty batch returns at once (batched.jl:285, 303).
  * Replaces solve_batch! (src/nonlinear/batched.jl:257-307).
  */
-int gsb_solve_batch(const GsbProblem* prob, const GsbMethod* method, const GsbOptions* opt,
+GSB_API int gsb_solve_batch(const GsbProblem* prob, const GsbMethod* method, const GsbOptions* opt,
                     double* X, int32_t x_layout, void* S, int32_t s_kind, const double* P,
                     int32_t p_layout, const int64_t* order, int32_t order_base, int64_t nsys,
                     void* stream, GsbTally* tally);
 
 /* batch_summary(S) of nsys device statuses into *out (host), src/nonlinear/batched.jl:80-89.
  * Synchronises `stream`. */
-int gsb_batch_summary(const GsbStatus64* S, int64_t nsys, void* stream, GsbSummary* out);
+GSB_API int gsb_batch_summary(const GsbStatus64* S, int64_t nsys, void* stream, GsbSummary* out);
 
 /* Wait for the work queued on `stream`. */
-int gsb_synchronize(void* stream);
+GSB_API int gsb_synchronize(void* stream);
 
 #ifdef __cplusplus
 }

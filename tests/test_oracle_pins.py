@@ -1,0 +1,273 @@
+"""The oracle pinned to the reference's own golden table and test assertions (CPU only).
+
+Pins (file:line within GeometricSolvers.jl):
+  test/verification/standard_reference.csv: Float64 rows of "Newton Static LU" and
+      "Newton Backtracking LU", compared as test/helpers/standard_cells.jl:377-399 compares them
+      (code exact, iterations within 1 on rows not flagged unstable/platform);
+  test/nonlinear/batched.jl:461-499 (six outcomes), :263-397 (exact dyadic root, singular start);
+  test/nonlinear/refinement.jl:466-632 (A_MOD, A_ILL) and :686-725 (Check 1);
+  test/globalization/linesearch.jl and backtracking.jl (the step rules);
+  src/linear/factors.jl:726-758 (ldexp2).
+"""
+
+import json
+import math
+import os
+
+import numpy as np
+import pytest
+
+from workloads import rng
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+NAMES = ["SUCCESS", "STALLED", "MAXITERS", "SINGULAR", "NONFINITE", "LINESEARCH_FAILED"]
+
+
+def _cells():
+    with open(os.path.join(HERE, "golden", "standard_newton_lu_f64.json")) as fh:
+        return json.load(fh)["cells"]
+
+
+@pytest.mark.parametrize("cell", _cells(), ids=lambda c: f"p{c['problem']}-{c['start']}-{c['column'].split()[1]}")
+def test_standard_table(cell, oracle):
+    col = 0 if cell["column"] == "Newton Static LU" else 1
+    x, st, f_evals, _ = oracle.standard_cell(cell["problem"], np.array(cell["x0"]), col, 200)
+    if cell["unstable"] or cell["platform"]:
+        # the reference compares such a cell only for its presence
+        return
+    assert NAMES[st.code] == cell["code"]
+    assert abs(st.iterations - cell["iterations"]) <= 1
+    # the restatement reproduces the stable rows exactly
+    assert st.iterations == cell["iterations"]
+    assert f_evals == cell["f_evals"]
+
+
+def test_standard_roots(oracle):
+    # test/verification/standard.jl:55-79: the stated roots and the hand residual of problem 1
+    y = oracle.standard_residual(1, np.array([-1.2] + [1.0] * 9))
+    assert np.allclose(y, [2.2, -4.4] + [0.0] * 8, rtol=8 * np.finfo(float).eps, atol=0)
+    for number, root in ((2, [0.0] * 4), (4, [1.0] * 4), (5, [1.0, 0.0, 0.0]), (8, [1.0] * 10),
+                         (12, [1.0] * 10), (17, [0.0, 3.0]), (20, [5.0]), (21, [5.0, 4.0]),
+                         (22, [0.0, 1.0])):
+        r = np.array(root)
+        y = oracle.standard_residual(number, r)
+        assert np.max(np.abs(y)) <= 100 * len(r) * np.finfo(float).eps * max(1, np.max(np.abs(r)))
+
+
+def _newton_bt(gsb):
+    return gsb.Newton(globalization=gsb.Backtracking())
+
+
+def test_six_outcomes(gsb, oracle):
+    codes = [1, 2, 3, 4, 5, 6, 1, 3]
+    X = np.array([[2.5, 3.5]] * 8)
+    P = np.array(codes, float)[:, None]
+    X1, S = oracle.solve_batch(gsb.NonlinearProblem(gsb.Hetero6()), _newton_bt(gsb), X, P,
+                               gsb.Options(max_iterations=3))
+    assert [NAMES[c] for c in S["code"]] == ["SUCCESS", "STALLED", "MAXITERS", "SINGULAR",
+                                             "NONFINITE", "LINESEARCH_FAILED", "SUCCESS",
+                                             "MAXITERS"]
+    _, codes_only = oracle.solve_batch(gsb.NonlinearProblem(gsb.Hetero6()), _newton_bt(gsb), X, P,
+                                       gsb.Options(max_iterations=3), s_kind="codes")
+    assert np.bincount(codes_only, minlength=6).tolist() == [2, 1, 2, 1, 1, 1]
+
+
+def test_exact_root_and_singular_start(gsb, oracle):
+    p = np.array([[2.125, 1.5], [1.25, 2.0], [1.5, 2.5], [1.75, 3.0]])
+    x0 = np.array([[2.0, 1.0], [2.5, 1.5], [3.5, 2.5], [4.0, 3.0]])
+    X, S = oracle.solve_batch(gsb.NonlinearProblem(gsb.Coupled2()), gsb.Newton(), x0.copy(), p,
+                              gsb.Options(max_iterations=150))
+    assert X[0].tolist() == [2.0, 1.0]
+    assert S["iterations"][0] == 0 and S["code"][0] == 0
+    assert all(S["iterations"][1:] > 0) and all(S["code"] == 0)
+    x0s = x0.copy()
+    x0s[1] = [4.0, 4.0]
+    _, S = oracle.solve_batch(gsb.NonlinearProblem(gsb.Coupled2()), gsb.Newton(), x0s, p,
+                              gsb.Options(max_iterations=60))
+    assert [NAMES[c] for c in S["code"]] == ["SUCCESS", "SINGULAR", "SUCCESS", "SUCCESS"]
+
+
+def test_order_permutation(gsb, oracle):
+    p = np.array([[2.125, 1.5], [1.25, 2.0], [1.5, 2.5], [1.75, 3.0]])
+    x0 = np.array([[2.0, 1.0], [2.5, 1.5], [3.5, 2.5], [4.0, 3.0]])
+    Xa, Sa = oracle.solve_batch(gsb.NonlinearProblem(gsb.Coupled2()), gsb.Newton(), x0.copy(), p)
+    Xb, Sb = oracle.solve_batch(gsb.NonlinearProblem(gsb.Coupled2()), gsb.Newton(), x0.copy(), p,
+                                order=[3, 1, 0, 2])
+    assert np.array_equal(Xa, Xb) and Sa.tobytes() == Sb.tobytes()
+
+
+def test_hostile_inputs(gsb, oracle):
+    # test/nonlinear/batched.jl:647-667: NaN and Inf starts give NONFINITE with 0 iterations; a
+    # subnormal start converges
+    from workloads import cubic_affine
+
+    X, P = cubic_affine(3, 4, 4.0, 9)
+    X[0, 0] = np.nan
+    X[1, 1] = np.inf
+    X[2, 2] = 5e-324
+    _, S = oracle.solve_batch(gsb.NonlinearProblem(gsb.CubicAffine(3)), _newton_bt(gsb), X, P,
+                              gsb.Options(f_abstol=1e-12, f_reltol=0.0, max_iterations=50))
+    assert S["code"].tolist()[:3] == [4, 4, 0]
+    assert S["iterations"][0] == 0 and S["iterations"][1] == 0
+
+
+def _quadmod(A):
+    A = np.array(A)
+    u = A @ np.array([1.0, 2.0])
+    b = np.array([u[0] + 0.1 * u[0] ** 2, u[1] - 0.2 * u[1] ** 2])
+    return np.concatenate([A.flatten(order="F"), b])[None, :]
+
+
+A_MOD = [[1.3, 1.1], [1.1, 1.1 * 1.1 / 1.3 + 2e-5]]
+A_ILL = [[1.0, 1.0], [1.0, 1.0 + 1e-7]]
+
+
+def _solve_quad(gsb, oracle, A, method):
+    opts = gsb.Options(f_abstol=1e-12, f_reltol=0.0)
+    X, S = oracle.solve_batch(None, method, np.array([[2.0, 3.0]]), _quadmod(A), opts,
+                              family_code=oracle.FAM_QUADMOD2, n=2, m=2)
+    return X[0], S[0]
+
+
+def test_mixed_refinement_moderate(gsb, oracle):
+    # refinement.jl:466-541: FP32 factor + Refinement matches FP64's iterations, no promotion
+    _, s64 = _solve_quad(gsb, oracle, A_MOD, gsb.Newton())
+    assert s64["code"] == 0
+    for L in (gsb.LUFactorization, gsb.QRFactorization):
+        x, s = _solve_quad(gsb, oracle, A_MOD, gsb.Newton(linsolve=L("float32"),
+                                                        refinement=gsb.Refinement()))
+        assert s["code"] == 0 and s["fnorm"] < 1e-11
+        assert not s["promoted"] and s["step_failures"] == 0
+        assert s["iterations"] == s64["iterations"]
+        assert np.linalg.norm(x - [1.0, 2.0]) < 1e-10
+        assert math.isfinite(s["gradratio"]) and s["gradratio"] > 0
+        assert s["rank"] == -1 and math.isnan(s["nullnorm"])
+
+
+def test_mixed_promotion_ill(gsb, oracle):
+    # refinement.jl:543-632: refinement fails on the FP32 factor and promotes within the step
+    for L in (gsb.LUFactorization, gsb.QRFactorization):
+        x, s = _solve_quad(gsb, oracle, A_ILL, gsb.Newton(linsolve=L("float32"),
+                                                        refinement=gsb.Refinement()))
+        assert s["code"] == 0 and s["promoted"] and s["step_failures"] == 1
+        assert s["fnorm"] < 1e-12 and np.linalg.norm(x - [1.0, 2.0]) < 1e-5
+    x, s = _solve_quad(gsb, oracle, A_ILL, gsb.Newton(linsolve=gsb.LUFactorization("float32")))
+    assert s["code"] == 0 and s["promoted"] and s["step_failures"] >= 1
+    assert np.linalg.norm(x - [1.0, 2.0]) < 1e-5
+
+
+def test_check1_mixed_keeps_going(gsb, oracle):
+    # refinement.jl:686-725 (Check 1), with this build's seeded generator in place of Xoshiro(7):
+    # FP32-LU keeps FP64's code and iterations, never STALLED, never promoted
+    g = rng(99)
+    P = []
+    X0 = []
+    for _ in range(30):
+        A = g.standard_normal((2, 2)) + 3 * np.eye(2)
+        c = g.standard_normal(2)
+        b = 5 * g.standard_normal(2)
+        P.append(np.concatenate([A.flatten(order="F"), c, b]))
+        X0.append(g.standard_normal(2))
+    P, X0 = np.array(P), np.array(X0)
+    opts = gsb.Options()
+    _, s64 = oracle.solve_batch(None, gsb.Newton(), X0.copy(), P, opts,
+                                family_code=oracle.FAM_CUBICDIAG2, n=2, m=2)
+    _, s32 = oracle.solve_batch(None, gsb.Newton(linsolve=gsb.LUFactorization("float32")),
+                                X0.copy(), P, opts, family_code=oracle.FAM_CUBICDIAG2, n=2, m=2)
+    # the two counts of Check 1 over all draws
+    assert np.count_nonzero(s32["code"] == 1) == 0
+    assert np.count_nonzero(s32["promoted"]) == 0
+    # its first assertion (same code and iterations as FP64) on the draws that FP64 solves
+    # quickly, as the reference's three first draws are; long runs wander chaotically
+    quick = (s64["code"] == 0) & (s64["iterations"] <= 12)
+    assert np.count_nonzero(quick) >= 10
+    assert np.array_equal(s32["code"][quick], s64["code"][quick])
+    assert np.array_equal(s32["iterations"][quick], s64["iterations"][quick])
+
+
+def test_backtracking_exact_step_needs_no_slope(oracle):
+    # linesearch.jl:179-193: the exact step evaluates no φ′, a measured slope one more
+    c = np.linspace(0.5, 3.0, 8)
+    phi = lambda a: float(np.sum(((1 - a) * c) ** 2))
+    dphi = lambda a: float(-2 * np.sum((1 - a) * c * c))
+    code, a, _, ev, _ = oracle.backtracking(phi, dphi, phi(0.0), exact=True)
+    code2, a2, _, ev2, _ = oracle.backtracking(phi, dphi, phi(0.0), exact=False)
+    assert code == 0 and code2 == 0
+    assert a2 == pytest.approx(a, rel=8 * np.finfo(float).eps)
+    assert ev2 == ev + 1
+
+
+def test_backtracking_roundoff_floor(oracle):
+    # linesearch.jl:756-771: the merit falls by `ulps` ulps at its minimiser; 2 ulps is the
+    # round-off floor (STALLED), 8 ulps a decrease (SUCCESS)
+    for ulps, code in ((2, 1), (8, 0)):
+        a_ = ulps * np.finfo(float).eps
+        phi = lambda t: 1.0 - 2 * a_ * t + a_ * t * t
+        dphi = lambda t: -2 * a_ + 2 * a_ * t
+        got, *_ = oracle.backtracking(phi, dphi, 1.0, exact=False)
+        assert got == code
+
+
+def test_backtracking_step_floor(oracle):
+    # linesearch.jl:420-433: φ = 1 - 2α + kα² accepts only α below 2/k; the Armijo test holds
+    for k in (1e10, 1e11, 1e12):
+        phi = lambda a: 1 - 2 * a + k * a * a
+        dphi = lambda a: -2 + 2 * k * a
+        for exact in (True, False):
+            code, a, p, _, _ = oracle.backtracking(phi, dphi, 1.0, exact=exact)
+            assert code == 0 and p - 1 <= -2 * 1e-4 * a
+
+
+def test_backtracking_frozen_trials(oracle):
+    # linesearch.jl:750-755: a merit equal to φ₀ bit for bit at steps below √eps is STALLED
+    o = 1.0
+    phi = lambda a: o if a <= 1e-6 else 1 + a
+    code, _, _, _, trials = oracle.backtracking(phi, lambda a: -2.0, 1.0, exact=False)
+    assert code == 1
+    assert sum(1 for a in trials if a <= math.sqrt(np.finfo(float).eps) and phi(a) == o) >= 2
+
+
+def test_backtrack_step_rules(oracle):
+    # backtracking.jl:62-82: a non-finite merit gives 0.1 α; the result lies in [0.1 α, p α]
+    assert oracle.lib().oracle_backtrack_step(1.0, -2.0, 1.0, math.inf, math.nan, math.nan, 0.5) == 0.1
+    for pa in (0.5, 0.99, 2.0, 10.0):
+        a = oracle.lib().oracle_backtrack_step(1.0, -2.0, 1.0, pa, math.nan, math.nan, 0.5)
+        assert 0.1 <= a <= 0.5
+
+
+def test_ldexp2_exact(oracle):
+    # factors.jl:726-758: exact in range, nearest-even into the subnormals, Inf above
+    assert oracle.ldexp2(1.5, 3) == 12.0
+    assert oracle.ldexp2(1.0, -1074) == 5e-324
+    assert oracle.ldexp2(1.0, -1075) == 0.0          # a tie rounds to even (zero)
+    assert oracle.ldexp2(1.5, -1075) == 5e-324       # above the tie rounds up
+    assert oracle.ldexp2(3.0, 1023) == math.inf
+    assert oracle.ldexp2(5e-324, 1074) == 1.0
+    assert math.isnan(oracle.ldexp2(math.nan, 5))
+    g = rng(5)
+    for v in g.standard_normal(200) * 1e-300:
+        for e in (-30, -10, 5, 40):
+            assert oracle.ldexp2(float(v), e) == math.ldexp(float(v), e)
+
+
+def test_scaled_solves(oracle):
+    # factors.jl:802-811, 880-885, 943-949: a tiny and a huge Jacobian solve to J \ r
+    g = rng(7)
+    for scale in (1e-300, 1.0, 1e300):
+        J = (g.standard_normal((4, 4)) + 4 * np.eye(4)) * scale
+        r = g.standard_normal(4) * scale
+        for qr in (False, True):
+            info, d, e = oracle.factor_solve(J, r, qr=qr)
+            assert info == 0
+            assert np.allclose(d, np.linalg.solve(J, r), rtol=1e-12)
+            info32, d32, _ = oracle.factor_solve(J, r, qr=qr, f32=True)
+            assert info32 == 0 and np.allclose(d32, d, rtol=1e-5)
+    info, _, _ = oracle.factor_solve(np.zeros((3, 3)), np.ones(3))
+    assert info == 1
+
+
+def test_givens(oracle):
+    c, s, r = oracle.givens(3.0, 4.0)
+    assert (c, s, r) == (0.6, 0.8, 5.0)
+    assert oracle.givens(2.0, 0.0) == (1.0, 0.0, 2.0)
+    assert oracle.givens(0.0, 2.0) == (0.0, 1.0, 2.0)

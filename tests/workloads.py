@@ -1,0 +1,46 @@
+"""Seeded synthetic inputs of the batch configurations (shared by the tests and bench.py).
+
+Counter-based generation with numpy's Philox bit generator, seed 20261203 + config id, so
+every rank and every run draws the same systems.
+"""
+
+import numpy as np
+
+SEED = 20261203
+
+
+def rng(config_id, stream=0):
+    return np.random.Generator(np.random.Philox(key=SEED + config_id, counter=stream))
+
+
+def cubic_affine(n, nsys, diag, config_id, stream=0):
+    """F(x) = A x + 0.1 x.^3 - b: A = diag I + 0.5 N(0,1), b ~ U(-1, 1)^n, x0 = 0.
+    Returns (X0 (nsys, n), P (nsys, n*n + n)) with A column-major in each parameter block."""
+    g = rng(config_id, stream)
+    A = g.standard_normal((nsys, n, n)) * 0.5
+    A[:, np.arange(n), np.arange(n)] += diag
+    b = g.uniform(-1.0, 1.0, (nsys, n))
+    P = np.concatenate([A.transpose(0, 2, 1).reshape(nsys, n * n), b], axis=1)
+    return np.zeros((nsys, n)), np.ascontiguousarray(P)
+
+
+def c0(nsys=65536):
+    return cubic_affine(3, nsys, 4.0, 0)
+
+
+def c1(nsys=1048576):
+    return cubic_affine(8, nsys, 6.0, 1)
+
+
+def cubic_affine_pivoting(n, nsys, diag, config_id):
+    """The cubic-affine batch with the rows of each A in a random order (b permuted alike), so
+    that partial pivoting exchanges rows in nearly every factorisation."""
+    X0, P = cubic_affine(n, nsys, diag, config_id)
+    g = rng(config_id, stream=7)
+    A = P[:, : n * n].reshape(nsys, n, n).transpose(0, 2, 1)  # back to row-major (nsys, n, n)
+    b = P[:, n * n:]
+    perm = np.argsort(g.random((nsys, n)), axis=1)
+    A = np.take_along_axis(A, perm[:, :, None], axis=1)
+    b = np.take_along_axis(b, perm, axis=1)
+    P = np.concatenate([A.transpose(0, 2, 1).reshape(nsys, n * n), b], axis=1)
+    return X0, np.ascontiguousarray(P)

@@ -163,6 +163,7 @@ EXPORTED_SYMBOLS = (
     "gsb_solve_batch",
     "gsb_batch_summary",
     "gsb_synchronize",
+    "gsb_solve_batch_counts_noalloc",
 )
 
 _lib = None
@@ -199,5 +200,12 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.gsb_batch_summary.restype = ctypes.c_int
     lib.gsb_synchronize.argtypes = [ctypes.c_void_p]
     lib.gsb_synchronize.restype = ctypes.c_int
+    lib.gsb_solve_batch_counts_noalloc.argtypes = [
+        P(GsbProblem), P(GsbMethod), P(GsbOptions),
+        ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p,
+        ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_int32,
+        ctypes.c_int64, ctypes.c_void_p, P(GsbTally),
+    ]
+    lib.gsb_solve_batch_counts_noalloc.restype = ctypes.c_int
     _lib = lib
     return lib

@@ -75,6 +75,37 @@ __global__ void summary_kernel(const unsigned char* S, int64_t nsys, SummaryAcc*
     }
 }
 
+
+// ─── the working memory of gsb_solve_batch_counts_noalloc ─────────────────────────────────
+// One static array per device that loads the library: words 0..5 are the six counters of the
+// count form, word 6 the error flags of the `order` check (1: an entry out of range, 2: an
+// entry seen twice), word 7 unused, and the rest one bit per system for that check.
+constexpr int kNoallocHead = 8;
+constexpr int64_t kNoallocBitmapWords = (int64_t)GSB_NOALLOC_MAX_ORDERED / 64;
+static __device__ __align__(256) unsigned long long g_noalloc_scratch[kNoallocHead + kNoallocBitmapWords];
+
+// Clears the counters, the flags and the first `words` bitmap words.
+__global__ void noalloc_clear(unsigned long long* scratch, int64_t words) {
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < kNoallocHead + words;
+         q += (int64_t)gridDim.x * blockDim.x)
+        scratch[q] = 0ull;
+}
+
+// Marks each entry of `order` in the bitmap and flags out-of-range and repeated entries.
+__global__ void noalloc_check_order(const int64_t* order, int order_base, int64_t nsys,
+                                    unsigned long long* scratch) {
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < nsys;
+         q += (int64_t)gridDim.x * blockDim.x) {
+        int64_t v = order[q] - order_base;
+        if (v < 0 || v >= nsys) {
+            atomicOr(scratch + 6, 1ull);
+            continue;
+        }
+        unsigned long long bit = 1ull << (v & 63);
+        unsigned long long old = atomicOr(scratch + kNoallocHead + (v >> 6), bit);
+        if (old & bit) atomicOr(scratch + 6, 2ull);
+    }
+}
 }  // namespace gsb
 
 using namespace gsb;
@@ -199,6 +230,72 @@ int check_method(const GsbMethod* m) {
         return set_err(GSB_ERR_UNSUPPORTED, "the batch path takes regularization = 0");
     if (m->arithmetic != GSB_FUSED && m->arithmetic != GSB_UNFUSED)
         return set_err(GSB_ERR_ARGUMENT, "arithmetic must be GSB_FUSED or GSB_UNFUSED");
+    return 0;
+}
+
+
+// The device address of g_noalloc_scratch on the current device, looked up once per device (a
+// host-side name of a __device__ array is not a device address). No allocation.
+std::mutex g_noalloc_mu;
+unsigned long long* g_noalloc_ptr[64] = {};
+
+int noalloc_scratch(unsigned long long** out) {
+    int dev = 0;
+    if (int rc = cuda_err(cudaGetDevice(&dev), "cudaGetDevice")) return rc;
+    if (dev < 0 || dev >= 64) return set_err(GSB_ERR_CUDA, "device index out of range");
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+        unsigned long long* p = nullptr;
+        if (int rc = cuda_err(cudaGetSymbolAddress(reinterpret_cast<void**>(&p), g_noalloc_scratch),
+                              "cudaGetSymbolAddress"))
+            return rc;
+        g_noalloc_ptr[dev] = p;
+    }
+    *out = g_noalloc_ptr[dev];
+    return 0;
+}
+
+// Pick the kernel for the call and launch it on `st` (arguments already checked).
+int launch_solve(const GsbProblem* prob, const GsbMethod* method, const GsbOptions* opt, double* X,
+                 int32_t x_layout, void* S, int32_t s_kind, const double* P, int32_t p_layout,
+                 const int64_t* order, int32_t order_base, int64_t nsys, cudaStream_t st,
+                 unsigned long long* tally_dev) {
+    if (method->globalization == GSB_LEVENBERG_MARQUARDT)
+        return set_err(GSB_ERR_UNSUPPORTED, "LevenbergMarquardt batch kernel not in this build");
+    if (method->linsolve != GSB_LU)
+        return set_err(GSB_ERR_UNSUPPORTED, "QRFactorization batch kernel not in this build");
+    const bool mixed = method->factor_precision == GSB_F32;
+    const bool fused = method->arithmetic == GSB_FUSED;
+    KernelEntry* ke = select_kernel(prob, fused, mixed);
+    if (!ke) return set_err(GSB_ERR_UNSUPPORTED, "no batch kernel for this family and size");
+    int dev = 0;
+    if (int rc = cuda_err(cudaGetDevice(&dev), "cudaGetDevice")) return rc;
+    size_t smem = (size_t)kThreads * ke->row * sizeof(double);
+    if (!ke->attr_set[dev & 63]) {
+        if (int rc = cuda_err(cudaFuncSetAttribute(reinterpret_cast<const void*>(ke->fn),
+                                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   (int)smem),
+                              "cudaFuncSetAttribute"))
+            return rc;
+        ke->attr_set[dev & 63] = true;
+    }
+    Launch L{X, x_layout, S, s_kind, P, p_layout, order, order_base, nsys, prob->shared, tally_dev};
+    int64_t blocks = (nsys + kThreads - 1) / kThreads;
+    ke->fn<<<(unsigned)blocks, kThreads, smem, st>>>(*method, *opt, L);
+    return cuda_err(cudaGetLastError(), "kernel launch");
+}
+
+// The argument checks of gsb_solve_batch, for the entry point that allocates nothing.
+int check_call(const GsbProblem* prob, const GsbMethod* method, const GsbOptions* opt,
+               int64_t nsys, int32_t x_layout, int32_t p_layout, int32_t order_base) {
+    if (!prob || !method || !opt) return set_err(GSB_ERR_ARGUMENT, "null problem, method or options");
+    if (nsys < 0) return set_err(GSB_ERR_DIMENSION, "negative batch length");
+    if (int rc = check_options(opt)) return rc;
+    if (int rc = check_method(method)) return rc;
+    if (param_count(prob) < 0) return set_err(GSB_ERR_ARGUMENT, "unknown family or size");
+    if (x_layout != GSB_AOS && x_layout != GSB_SOA) return set_err(GSB_ERR_ARGUMENT, "x_layout");
+    if (p_layout != GSB_AOS && p_layout != GSB_SOA) return set_err(GSB_ERR_ARGUMENT, "p_layout");
+    if (order_base != 0 && order_base != 1) return set_err(GSB_ERR_ARGUMENT, "order_base");
     return 0;
 }
 
@@ -386,6 +483,54 @@ int gsb_batch_summary(const GsbStatus64* S, int64_t nsys, void* stream, GsbSumma
 int gsb_synchronize(void* stream) {
     return cuda_err(cudaStreamSynchronize(reinterpret_cast<cudaStream_t>(stream)),
                     "cudaStreamSynchronize");
+}
+
+
+int gsb_solve_batch_counts_noalloc(const GsbProblem* prob, const GsbMethod* method,
+                                   const GsbOptions* opt, double* X, int32_t x_layout,
+                                   uint8_t* codes, const double* P, int32_t p_layout,
+                                   const int64_t* order, int32_t order_base, int64_t nsys,
+                                   void* stream, GsbTally* tally) {
+    g_err.clear();
+    if (!tally) return set_err(GSB_ERR_ARGUMENT, "the count form needs a host GsbTally");
+    std::memset(tally, 0, sizeof(*tally));
+    if (int rc = check_call(prob, method, opt, nsys, x_layout, p_layout, order_base)) return rc;
+    if (order && nsys > (int64_t)GSB_NOALLOC_MAX_ORDERED)
+        return set_err(GSB_ERR_DIMENSION,
+                       "with an order, the allocation-free count form takes at most "
+                       "16777216 systems (GSB_NOALLOC_MAX_ORDERED)");
+    if (nsys == 0) return 0;
+    if (!X || !codes || !P) return set_err(GSB_ERR_ARGUMENT, "null X, codes or P");
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    unsigned long long* scratch = nullptr;
+    if (int rc = noalloc_scratch(&scratch)) return rc;
+    const int64_t words = order ? (nsys + 63) / 64 : 0;
+    noalloc_clear<<<(unsigned)((kNoallocHead + words + 255) / 256 > 1184 ? 1184 : (kNoallocHead + words + 255) / 256),
+                    256, 0, st>>>(scratch, words);
+    if (int rc = cuda_err(cudaGetLastError(), "noalloc_clear")) return rc;
+    if (order) {
+        // isperm on the device (the reference checks it on the host,
+        // src/nonlinear/batched.jl:134-136)
+        unsigned blocks = (unsigned)((nsys + 255) / 256 > 1184 ? 1184 : (nsys + 255) / 256);
+        noalloc_check_order<<<blocks, 256, 0, st>>>(order, order_base, nsys, scratch);
+        if (int rc = cuda_err(cudaGetLastError(), "noalloc_check_order")) return rc;
+        unsigned long long flags = 0;
+        if (int rc = cuda_err(cudaMemcpyAsync(&flags, scratch + 6, sizeof(flags),
+                                              cudaMemcpyDeviceToHost, st), "flag copy"))
+            return rc;
+        if (int rc = cuda_err(cudaStreamSynchronize(st), "flag copy")) return rc;
+        if (flags) return set_err(GSB_ERR_ARGUMENT, "order is not a permutation of the batch");
+    }
+    if (int rc = launch_solve(prob, method, opt, X, x_layout, codes, GSB_CODES, P, p_layout, order,
+                              order_base, nsys, st, scratch))
+        return rc;
+    unsigned long long h[6];
+    if (int rc = cuda_err(cudaMemcpyAsync(h, scratch, sizeof(h), cudaMemcpyDeviceToHost, st),
+                          "tally copy"))
+        return rc;
+    if (int rc = cuda_err(cudaStreamSynchronize(st), "tally copy")) return rc;
+    for (int c = 0; c < 6; ++c) tally->counts[c] = (int64_t)h[c];
+    return 0;
 }
 
 }  // extern "C"

@@ -242,6 +242,31 @@ GSB_API int gsb_batch_summary(const GsbStatus64* S, int64_t nsys, void* stream, 
 /* Wait for the work queued on `stream`. */
 GSB_API int gsb_synchronize(void* stream);
 
+/*
+ * The count form of gsb_solve_batch for callers that cannot allocate device memory: a host whose
+ * memory manager has reserved the whole device heap for its own pool, or a loop that cannot take
+ * the device-wide synchronisation of cudaMalloc. No counterpart in the reference: it is the count
+ * form (src/nonlinear/batched.jl:289-307) with its working memory moved out of the allocator.
+ *
+ * It solves in place like gsb_solve_batch with s_kind GSB_CODES: X receives the iterates, `codes`
+ * (uint8_t[nsys], device) the ReturnCodes, and *tally (host, required) the six counts. The six
+ * counters and the permutation check of `order` live in one static device array of this library
+ * (2 MiB, held by every device that loads the library until the process exits), so the call
+ * allocates nothing: no cudaMalloc, no host heap. Limit: with `order`, nsys may be at most
+ * GSB_NOALLOC_MAX_ORDERED (16,777,216); beyond it the call returns GSB_ERR_DIMENSION before any
+ * launch. Without `order` there is no limit. The first call on a device also looks up the
+ * array's device address; make that first call before any stream capture on that device. Every
+ * call reuses the same array (each call clears what it needs first), so calls that overlap on
+ * the device race: issue them on one stream, or wait between them. The call returns after its
+ * counts have reached the host.
+ */
+#define GSB_NOALLOC_MAX_ORDERED 16777216
+GSB_API int gsb_solve_batch_counts_noalloc(const GsbProblem* prob, const GsbMethod* method,
+                                           const GsbOptions* opt, double* X, int32_t x_layout,
+                                           uint8_t* codes, const double* P, int32_t p_layout,
+                                           const int64_t* order, int32_t order_base,
+                                           int64_t nsys, void* stream, GsbTally* tally);
+
 #ifdef __cplusplus
 }
 #endif

@@ -127,7 +127,7 @@ class GsbMethod(ctypes.Structure):
         ("lm_rho_accept", ctypes.c_double),
         ("regularization", ctypes.c_double),
         ("arithmetic", ctypes.c_int32),
-        ("pad_", ctypes.c_int32),
+        ("threads_per_system", ctypes.c_int32),
     ]
 
 

@@ -216,10 +216,15 @@ class Newton:
     # The rounding of the linear algebra on the device: "fused" (FMA, the default) or
     # "unfused" (every product and sum rounded alone, as Julia evaluates); no reference field.
     arithmetic: str = "fused"
+    # Lanes of a warp that share one system on the device (1, 2, 4, 8, 16, 32), or None for the
+    # library's tuned choice; no reference field.
+    threads_per_system: Optional[int] = None
 
     def __post_init__(self):
         if self.arithmetic not in ("fused", "unfused"):
             raise ArgumentError("arithmetic must be 'fused' or 'unfused'")
+        if self.threads_per_system not in (None, 1, 2, 4, 8, 16, 32):
+            raise ArgumentError("threads_per_system must be None or one of 1, 2, 4, 8, 16, 32")
         if isinstance(self.refinement, bool):
             object.__setattr__(self, "refinement", Refinement() if self.refinement else NoRefinement())
         if not (self.regularization >= 0 and math.isfinite(self.regularization)):
@@ -274,6 +279,7 @@ class Newton:
             raise ArgumentError("the batch path takes no factor reuse")
         m.regularization = 0.0
         m.arithmetic = abi.GSB_FUSED if self.arithmetic == "fused" else abi.GSB_UNFUSED
+        m.threads_per_system = 0 if self.threads_per_system is None else self.threads_per_system
         return m
 
 

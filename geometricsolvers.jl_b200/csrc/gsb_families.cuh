@@ -26,11 +26,9 @@ template <int N_> struct CubicAffine {
     struct JState {
         double diag[N];
     };
-    // A volatile read: the block stays in shared memory and is read at each use, rather than
-    // hoisted out of the Newton loop into registers, which the factor needs.
-    __device__ __forceinline__ double par(int k) const {
-        return *reinterpret_cast<const volatile double*>(p + k);
-    }
+    // The block stays in shared memory and is read at each use (a volatile shared load), rather
+    // than hoisted out of the Newton loop into registers, which the factor needs.
+    __device__ __forceinline__ double par(int k) const { return lds(smem_addr(p) + 8u * k); }
     __device__ __forceinline__ double A(int i, int k) const { return par(i + k * N); }
     __device__ __forceinline__ void F(const double (&x)[N], double (&out)[M]) const {
 #pragma unroll

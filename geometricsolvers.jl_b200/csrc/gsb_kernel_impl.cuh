@@ -9,6 +9,7 @@
 #include "gsb_families.cuh"
 #include "gsb_newton.cuh"
 #include "gsb_numerics.cuh"
+#include "gsb_team.cuh"
 
 namespace gsb {
 
@@ -67,8 +68,41 @@ __device__ __forceinline__ void tally_code(unsigned long long* tally, int code) 
     }
 }
 
-template <class Fam, bool F, bool Mixed>
-__global__ void __launch_bounds__(kThreads) newton_kernel(GsbMethod m, GsbOptions o, Launch L) {
+// Stage the contiguous AoS parameter chunk of a CTA (`rows` blocks of NP doubles from src) into
+// rows of stride RS in shared memory. Each thread issues all of its loads before any store, in
+// batches of 16, so that the HBM round trips of one thread overlap instead of following one
+// another.
+template <int NP, int RS, int ROWS>
+__device__ __forceinline__ void stage_aos(double* smem, const double* src, int64_t rows_left, int tid) {
+    constexpr int TOTAL = ROWS * NP;
+    constexpr int PER = (TOTAL + kThreads - 1) / kThreads;
+    constexpr int BATCH = 16;
+    const int total = rows_left < ROWS ? (int)rows_left * NP : TOTAL;
+#pragma unroll
+    for (int b0 = 0; b0 < PER; b0 += BATCH) {
+        double v[BATCH];
+#pragma unroll
+        for (int b = 0; b < BATCH; ++b) {
+            const int q = (b0 + b) * kThreads + tid;
+            v[b] = (b0 + b < PER && q < total) ? __ldg(src + q) : 0.0;
+        }
+#pragma unroll
+        for (int b = 0; b < BATCH; ++b) {
+            const int q = (b0 + b) * kThreads + tid;
+            if (b0 + b < PER && q < total) {
+                const int s = q / NP;
+                smem[s * RS + (q - s * NP)] = v[b];
+            }
+        }
+    }
+}
+
+#ifndef GSB_MIN_BLOCKS
+#define GSB_MIN_BLOCKS 1
+#endif
+
+template <class Fam, bool F, bool Mixed, bool PlainRef>
+__global__ void __launch_bounds__(kThreads, GSB_MIN_BLOCKS) newton_kernel(GsbMethod m, GsbOptions o, Launch L) {
     extern __shared__ double smem[];
     constexpr int N = Fam::N, NP = Fam::NP, RS = row_stride(NP, N);
     const int tid = threadIdx.x;
@@ -76,14 +110,7 @@ __global__ void __launch_bounds__(kThreads) newton_kernel(GsbMethod m, GsbOption
     const int64_t i = base + tid;
     double* prow = smem + tid * RS;
     if (L.order == nullptr && L.p_layout == GSB_AOS) {
-        int64_t rem = L.nsys - base;
-        int nloc = rem < (int64_t)blockDim.x ? (int)rem : (int)blockDim.x;
-        const double* src = L.P + base * NP;
-        for (int q = tid; q < nloc * NP; q += blockDim.x) {
-            int s = q / NP;
-            int k = q - s * NP;
-            smem[s * RS + k] = __ldg(src + q);
-        }
+        stage_aos<NP, RS, kThreads>(smem, L.P + base * NP, L.nsys - base, tid);
     } else if (i < L.nsys) {
         int64_t idx = L.order ? L.order[i] - L.order_base : i;
         if (L.p_layout == GSB_SOA) {
@@ -102,7 +129,7 @@ __global__ void __launch_bounds__(kThreads) newton_kernel(GsbMethod m, GsbOption
 #pragma unroll
     for (int k = 0; k < N; ++k)
         x[k] = L.x_layout == GSB_SOA ? L.X[(int64_t)k * L.nsys + idx] : L.X[idx * N + k];
-    Solver<Fam, F, Mixed> sv(fam, m, o, N >= 6 ? prow + NP : nullptr);
+    Solver<Fam, F, Mixed, PlainRef> sv(fam, m, o, N >= 6 ? prow + NP : nullptr);
     double gr;
     DevStatus s = sv.solve(x, gr);
 #pragma unroll
@@ -115,27 +142,94 @@ __global__ void __launch_bounds__(kThreads) newton_kernel(GsbMethod m, GsbOption
     if (L.tally) tally_code(L.tally, s.code);
 }
 
+
+// The team form: T lanes per system, kThreads / T systems per CTA, each system's parameter block
+// staged into a shared-memory row that its lanes read.
+template <class Fam, int T, bool Mixed>
+__global__ void __launch_bounds__(kThreads) team_kernel(GsbMethod m, GsbOptions o, Launch L) {
+    extern __shared__ double smem[];
+    constexpr int N = Fam::N, NP = Fam::NP, RS = (NP % 2 == 1) ? NP : NP + 1;
+    constexpr int SPB = kThreads / T;
+    const int tid = threadIdx.x;
+    const int team = tid / T;
+    const int64_t base = (int64_t)blockIdx.x * SPB;
+    const int64_t i = base + team;
+    if (L.order == nullptr && L.p_layout == GSB_AOS) {
+        stage_aos<NP, RS, SPB>(smem, L.P + base * NP, L.nsys - base, tid);
+    } else if (i < L.nsys) {
+        const int64_t idx = L.order ? L.order[i] - L.order_base : i;
+        double* prow = smem + team * RS;
+        for (int k = tid % T; k < NP; k += T)
+            prow[k] = L.p_layout == GSB_SOA ? __ldg(L.P + (int64_t)k * L.nsys + idx)
+                                            : __ldg(L.P + idx * NP + k);
+    }
+    __syncthreads();
+    if (i >= L.nsys) return;
+    const int64_t idx = L.order ? L.order[i] - L.order_base : i;
+    Fam fam{smem + team * RS};
+    double x[N];
+#pragma unroll
+    for (int k = 0; k < N; ++k)
+        x[k] = L.x_layout == GSB_SOA ? L.X[(int64_t)k * L.nsys + idx] : L.X[idx * N + k];
+    TeamSolver<Fam, T, Mixed> sv(fam, m, o);
+    double gr;
+    DevStatus s = sv.solve(x, gr);
+    const int lane = tid % T;
+#pragma unroll
+    for (int q = 0; q < N / T; ++q) {
+        const int k = q * T + lane;
+        const double v = own<N, T>(x, q, lane);
+        if (L.x_layout == GSB_SOA) L.X[(int64_t)k * L.nsys + idx] = v;
+        else L.X[idx * N + k] = v;
+    }
+    if (lane == 0) {
+        if (L.s_kind == GSB_STATUS64) store_status(L.S, idx, s, gr);
+        else reinterpret_cast<unsigned char*>(L.S)[idx] = (unsigned char)s.code;
+        if (L.tally) tally_code(L.tally, s.code);
+    }
+}
+
 using KernelFn = void (*)(GsbMethod, GsbOptions, Launch);
 
 struct KernelEntry {
     KernelFn fn;
-    int row;  // doubles of shared memory per thread
+    int smem_doubles;  // dynamic shared memory of a CTA, in doubles
+    int systems_per_block;
     bool attr_set[64];
 };
 
-template <class Fam, bool F, bool Mixed> KernelEntry* entry() {
-    static KernelEntry e{newton_kernel<Fam, F, Mixed>, row_stride(Fam::NP, Fam::N), {}};
+template <class Fam, bool F, bool Mixed, bool PlainRef> KernelEntry* entry() {
+    static KernelEntry e{newton_kernel<Fam, F, Mixed, PlainRef>,
+                         kThreads * row_stride(Fam::NP, Fam::N), kThreads, {}};
     return &e;
 }
 
-// The four kernels of a family: arithmetic fused or unfused, factor Float64 or Float32.
-template <class Fam> KernelEntry* pick(bool fused, bool mixed) {
-    if (fused) return mixed ? entry<Fam, true, true>() : entry<Fam, true, false>();
-    return mixed ? entry<Fam, false, true>() : entry<Fam, false, false>();
+template <class Fam, int T, bool Mixed> KernelEntry* team_entry() {
+    constexpr int RS = (Fam::NP % 2 == 1) ? Fam::NP : Fam::NP + 1;
+    static KernelEntry e{team_kernel<Fam, T, Mixed>, (kThreads / T) * RS, kThreads / T, {}};
+    return &e;
 }
 
-#define GSB_DECLARE_ENTRY(NAME) KernelEntry* entry_##NAME(bool fused, bool mixed)
-#define GSB_DEFINE_ENTRY(NAME, ...) \
-    KernelEntry* entry_##NAME(bool fused, bool mixed) { return pick<__VA_ARGS__>(fused, mixed); }
+template <class Fam, int T> KernelEntry* pick_team(bool mixed) {
+    return mixed ? team_entry<Fam, T, true>() : team_entry<Fam, T, false>();
+}
+
+// The six kernels of a family: arithmetic fused or unfused; factor Float32, or Float64 with or
+// without refinement.
+template <class Fam> KernelEntry* pick(bool fused, bool mixed, bool refine) {
+    if (fused) {
+        if (mixed) return entry<Fam, true, true, false>();
+        return refine ? entry<Fam, true, false, true>() : entry<Fam, true, false, false>();
+    }
+    if (mixed) return entry<Fam, false, true, false>();
+    return refine ? entry<Fam, false, false, true>() : entry<Fam, false, false, false>();
+}
+
+#define GSB_DECLARE_ENTRY(NAME) KernelEntry* entry_##NAME(bool fused, bool mixed, bool refine)
+#define GSB_DECLARE_TEAM(NAME) KernelEntry* team_##NAME(int T, bool mixed)
+#define GSB_DEFINE_ENTRY(NAME, ...)                                          \
+    KernelEntry* entry_##NAME(bool fused, bool mixed, bool refine) {         \
+        return pick<__VA_ARGS__>(fused, mixed, refine);                      \
+    }
 
 }  // namespace gsb

@@ -217,7 +217,10 @@ template <bool F, int N, class TF> struct LUFactor {
     }
 };
 
-template <class Fam, bool F, bool Mixed> struct Solver {
+// PlainRef: the plain (TF = T) step refines its direction (Refinement with a Float64 factor), a
+// rare configuration kept in its own instantiation so the common plain step holds no refinement
+// state in registers.
+template <class Fam, bool F, bool Mixed, bool PlainRef = false> struct Solver {
     static constexpr int N = Fam::N, M = Fam::M;
     using JS = typename Fam::JState;
     using A = Arith<F>;
@@ -233,23 +236,29 @@ template <class Fam, bool F, bool Mixed> struct Solver {
     // a volatile store and a volatile load, so that their register copies are free meanwhile.
     __device__ __forceinline__ void park(double (&x)[N], double (&Fx)[M]) const {
         if (stash == nullptr) return;
-        volatile double* v = stash;
+        const unsigned a = smem_addr(stash);
 #pragma unroll
-        for (int i = 0; i < N; ++i) v[i] = x[i];
+        for (int i = 0; i < N; ++i) sts(a + 8u * i, x[i]);
 #pragma unroll
-        for (int i = 0; i < M; ++i) v[N + i] = Fx[i];
+        for (int i = 0; i < M; ++i) sts(a + 8u * (N + i), Fx[i]);
+    }
+    __device__ __forceinline__ void park_x(const double (&x)[N]) const {
+        if (stash == nullptr) return;
+        const unsigned a = smem_addr(stash);
+#pragma unroll
+        for (int i = 0; i < N; ++i) sts(a + 8u * i, x[i]);
     }
     __device__ __forceinline__ void unpark_x(double (&x)[N]) const {
         if (stash == nullptr) return;
-        volatile double* v = stash;
+        const unsigned a = smem_addr(stash);
 #pragma unroll
-        for (int i = 0; i < N; ++i) x[i] = v[i];
+        for (int i = 0; i < N; ++i) x[i] = lds(a + 8u * i);
     }
     __device__ __forceinline__ void unpark_F(double (&Fx)[M]) const {
         if (stash == nullptr) return;
-        volatile double* v = stash;
+        const unsigned a = smem_addr(stash);
 #pragma unroll
-        for (int i = 0; i < M; ++i) Fx[i] = v[N + i];
+        for (int i = 0; i < M; ++i) Fx[i] = lds(a + 8u * (N + i));
     }
 
     __device__ __forceinline__ bool has_merit() const { return m.globalization == GSB_BACKTRACKING; }
@@ -493,27 +502,28 @@ template <class Fam, bool F, bool Mixed> struct Solver {
     // `failed`.
     template <class Fac>
     __device__ bool refine(double (&d)[N], const Fac& fac, const JS& js, const double (&Fx)[M]) const {
-        double fnorm = rnorm<F, M>(Fx);
+        const double fnorm = rnorm<F, M>(Fx);
         if (fnorm == 0.0) return false;
         if (!isfin(fnorm)) return true;
-        double eta = jmax(m.refine_eta, kSqrtEps);
-        double thr = __dmul_rn(eta, fnorm);
-        double Jv[N], r[N];
-        jmul(js, d, Jv);
+        const double thr = __dmul_rn(jmax(m.refine_eta, kSqrtEps), fnorm);
+        // r = -F - J d, formed in place of the product
+        double r[N];
+        jmul(js, d, r);
 #pragma unroll
-        for (int i = 0; i < N; ++i) r[i] = __dadd_rn(-Fx[i], -Jv[i]);
+        for (int i = 0; i < N; ++i) r[i] = __dadd_rn(-Fx[i], -r[i]);
         double rprev = rnorm<F, N>(r);
         if (!isfin(rprev)) return true;
         if (rprev <= thr) return false;
         for (int it = 1; it <= m.refine_maxiter; ++it) {
-            double dd[N], dc[N];
-            fac.ldiv(r, dd);
+            // the candidate d + fac \ r, formed in place of the correction
+            double dc[N];
+            fac.ldiv(r, dc);
 #pragma unroll
-            for (int i = 0; i < N; ++i) dc[i] = __dadd_rn(d[i], dd[i]);
-            jmul(js, dc, Jv);
+            for (int i = 0; i < N; ++i) dc[i] = __dadd_rn(d[i], dc[i]);
+            jmul(js, dc, r);
 #pragma unroll
-            for (int i = 0; i < N; ++i) r[i] = __dadd_rn(-Fx[i], -Jv[i]);
-            double rc = rnorm<F, N>(r);
+            for (int i = 0; i < N; ++i) r[i] = __dadd_rn(-Fx[i], -r[i]);
+            const double rc = rnorm<F, N>(r);
             if (!(rc < rprev)) return true;
 #pragma unroll
             for (int i = 0; i < N; ++i) d[i] = dc[i];
@@ -531,7 +541,7 @@ template <class Fam, bool F, bool Mixed> struct Solver {
         double gr, jn;
         grad_ratio_and_norm(js, Fx, fnorm, gr, jn);
         double merit = st.merit;
-        const bool ref = m.refinement == GSB_REFINEMENT;
+        constexpr bool ref = PlainRef;
         {
             park(x, Fx);
             LUFactor<F, N, double> fac;
@@ -546,7 +556,7 @@ template <class Fam, bool F, bool Mixed> struct Solver {
                 fac.ldiv(Fx, d);
 #pragma unroll
                 for (int i = 0; i < N; ++i) d[i] = -d[i];
-                if (ref) refine(d, fac, js, Fx);
+                if constexpr (ref) refine(d, fac, js, Fx);
                 unpark_x(x);
                 globalize(x, Fx, d, !ref, merit, info);
             }
@@ -576,6 +586,7 @@ template <class Fam, bool F, bool Mixed> struct Solver {
         double lin_rel = 0.0;
         bool md_promoted = was_promoted;
         bool fallback = was_promoted;
+        park_x(x);
         if (!was_promoted) {
             LUFactor<F, N, float> fac;
             fac.factor(fam, js);
@@ -618,6 +629,7 @@ template <class Fam, bool F, bool Mixed> struct Solver {
                 if (was_promoted && ref) refine(d, ft, js, Fx);
             }
         }
+        unpark_x(x);
         if (!ok) {
             st.promoted = md_promoted;
             info = {SINGULAR, rnorm<F, M>(Fx), 0.0, failures, md_promoted, false, false};

@@ -145,6 +145,22 @@ __device__ __forceinline__ float scale2_in(float x, int e) {
     return __fmul_rn(x, pow2f(e));
 }
 
+// Loads and stores of shared memory by its 32-bit shared-window address, as volatile PTX: the
+// compiler keeps them where they stand (a parameter block is read at each use instead of being
+// held in registers across the solve) and they issue as shared-memory instructions, not as
+// generic loads through the L1 path.
+__device__ __forceinline__ unsigned smem_addr(const void* p) {
+    return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ double lds(unsigned addr) {
+    double v;
+    asm volatile("ld.shared.f64 %0, [%1];" : "=d"(v) : "r"(addr));
+    return v;
+}
+__device__ __forceinline__ void sts(unsigned addr, double v) {
+    asm volatile("st.shared.f64 [%0], %1;" ::"r"(addr), "d"(v) : "memory");
+}
+
 // Julia's `exponent` of a finite nonzero value.
 __device__ __forceinline__ int jexponent(double x) { return ilogb(x); }
 __device__ __forceinline__ int jexponent(float x) { return ilogbf(x); }

@@ -151,7 +151,8 @@ typedef enum {
  *                                  LevenbergMarquardt(mu0, mu_min, mu_max, mu_decrease,
  *                                                     mu_increase, rho_accept; scaling = :none)
  * regularization must be 0 (the default); reuse, DogLeg and the matrix-free methods are not
- * part of this ABI. `arithmetic` has no counterpart in the reference (see GsbArithmetic).
+ * part of this ABI. `arithmetic` and `threads_per_system` have no counterpart in the reference:
+ * they choose the device arithmetic (GsbArithmetic) and how many lanes solve one system.
  */
 typedef struct {
     int32_t linsolve;         /* GsbLinsolve */
@@ -171,8 +172,9 @@ typedef struct {
     double lm_mu_increase;
     double lm_rho_accept;
     double regularization;
-    int32_t arithmetic;       /* GsbArithmetic */
-    int32_t pad_;
+    int32_t arithmetic;         /* GsbArithmetic */
+    int32_t threads_per_system; /* lanes of a warp that share one system: 1, 2, 4, 8, 16 or 32;
+                                   0 = the library's tuned choice for the family and size */
 } GsbMethod;
 
 /* The six counts of the count form, src/nonlinear/batched.jl:197-199, by GsbReturnCode. */

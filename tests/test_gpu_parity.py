@@ -137,6 +137,27 @@ def test_pivoting(gsb, oracle, n):
                          iterations=(arith == "unfused" or not mixed))
 
 
+@pytest.mark.parametrize("n,T", [(6, 2), (8, 2), (8, 4), (8, 8)])
+@pytest.mark.parametrize("pivoting", [False, True])
+def test_team_parity(gsb, oracle, n, T, pivoting):
+    # T lanes per system: identical codes and iterations on the plain path, rel err <= 1e-10
+    gen = cubic_affine_pivoting if pivoting else cubic_affine
+    X0, P = gen(n, 40000, n - 1.0, 11)
+    prob = gsb.NonlinearProblem(gsb.CubicAffine(n))
+    opts = gsb.Options(**OPTS)
+    for mixed in (False, True):
+        kw = dict(linsolve=gsb.LUFactorization("float32"), refinement=gsb.Refinement()) if mixed else {}
+        m = gsb.Newton(globalization=gsb.Backtracking(), threads_per_system=T, **kw)
+        xg, sg = run_gpu(gsb, prob, m, X0, P, opts)
+        xo, so = oracle.solve_batch(prob, m, X0.copy(), P, opts)
+        check_parity(xg, sg, xo, so, bitwise=False, iterations=not mixed)
+    for glob in (gsb.Static(),):
+        m = gsb.Newton(globalization=glob, threads_per_system=T)
+        xg, sg = run_gpu(gsb, prob, m, X0, P, opts)
+        xo, so = oracle.solve_batch(prob, m, X0.copy(), P, opts)
+        check_parity(xg, sg, xo, so, bitwise=False)
+
+
 def test_six_outcomes_and_count_form(gsb, oracle):
     codes = [1, 2, 3, 4, 5, 6, 1, 3]
     X0 = np.array([[2.5, 3.5]] * 8)

@@ -7,6 +7,7 @@
 // promotion to Float64 of src/nonlinear/newton.jl:1604-1720), globalization Static or
 // Backtracking. Status fields, codes and every stopping test follow the reference.
 #pragma once
+#include <type_traits>
 
 #include "../../include/gsb.h"
 #include "gsb_families.cuh"
@@ -214,6 +215,105 @@ template <bool F, int N, class TF> struct LUFactor {
                 for (int i = 0; i < N; ++i) d[i] = ldexp2_slow(d[i], E);
             }
         }
+    }
+};
+
+// The Float64 factorisation of the mixed step's rare branches (a promoted system, or the
+// promotion of a failed Float32 step), with its matrix in thread-local memory instead of
+// registers: the same operations in the same order as LUFactor<F, N, double> (lu.jl:24-64,
+// factors.jl:802-811, 931-936), so its results are identical, while the mixed kernel's register
+// budget is set by the Float32 factor it runs at every step. The loops keep runtime indices so
+// that the matrix stays in memory (L1-cached) rather than in registers.
+template <bool F, int N> struct LocalLU {
+    double a[N * N];
+    int ipiv[N];
+    int info;
+    int e;
+
+    template <class Fam, class JS>
+    __device__ __noinline__ void factor(const Fam& fam, const JS& js) {
+#pragma unroll
+        for (int k = 0; k < N; ++k)
+#pragma unroll
+            for (int i = 0; i < N; ++i) a[i + k * N] = fam.J(js, i, k);
+        e = matrix_exponent<N * N>(a);
+        if (e < 0) {
+#pragma unroll 1
+            for (int q = 0; q < N * N; ++q) a[q] = scale2_in(a[q], -e);  // -e in [1, 1023]
+        } else {
+            e = 0;
+        }
+        info = 0;
+#pragma unroll 1
+        for (int k = 0; k < N; ++k) {
+            int p = k;
+            double amax = fabs(a[k + k * N]);
+#pragma unroll 1
+            for (int i = k + 1; i < N; ++i) {
+                double v = fabs(a[i + k * N]);
+                if (v > amax) {
+                    amax = v;
+                    p = i;
+                }
+            }
+            ipiv[k] = p;
+            if (p != k) {
+#pragma unroll 1
+                for (int j = 0; j < N; ++j) {
+                    double t = a[k + j * N];
+                    a[k + j * N] = a[p + j * N];
+                    a[p + j * N] = t;
+                }
+            }
+            double akk = a[k + k * N];
+            if (akk == 0.0) {
+                if (info == 0) info = k + 1;
+            } else {
+#pragma unroll 1
+                for (int i = k + 1; i < N; ++i) a[i + k * N] = a[i + k * N] / akk;
+#pragma unroll 1
+                for (int j = k + 1; j < N; ++j)
+#pragma unroll 1
+                    for (int i = k + 1; i < N; ++i)
+                        a[i + j * N] = Arith<F>::msub(a[i + k * N], a[k + j * N], a[i + j * N]);
+            }
+        }
+    }
+
+    __device__ __noinline__ void backsolve(double* x) const {
+#pragma unroll 1
+        for (int k = 0; k < N; ++k) {
+            int p = ipiv[k];
+            if (p != k) {
+                double t = x[k];
+                x[k] = x[p];
+                x[p] = t;
+            }
+        }
+#pragma unroll 1
+        for (int k = 0; k < N; ++k) {
+            double xk = x[k];
+#pragma unroll 1
+            for (int i = k + 1; i < N; ++i) x[i] = Arith<F>::msub(a[i + k * N], xk, x[i]);
+        }
+#pragma unroll 1
+        for (int k = N - 1; k >= 0; --k) {
+            double xk = x[k] / a[k + k * N];
+            x[k] = xk;
+#pragma unroll 1
+            for (int i = 0; i < k; ++i) x[i] = Arith<F>::msub(a[i + k * N], xk, x[i]);
+        }
+    }
+
+    __device__ __forceinline__ void ldiv(const double (&r)[N], double (&d)[N]) const {
+        int k = rhs_exponent<N>(r, e);
+        double x[N];
+#pragma unroll
+        for (int i = 0; i < N; ++i) x[i] = k == 0 ? r[i] : scale2_in(r[i], -k);  // -k in [-6, 1023]
+        backsolve(x);
+        int e2 = k - e;
+#pragma unroll
+        for (int i = 0; i < N; ++i) d[i] = e2 == 0 ? x[i] : scale2_in(x[i], e2);  // e2 in [0, 1029]
     }
 };
 
@@ -618,7 +718,9 @@ template <class Fam, bool F, bool Mixed, bool PlainRef = false> struct Solver {
         if (fallback) {
             // the factorisation in the working precision: at every step once promoted (with the
             // refinement passes), and as the promotion of a failed Float32 step (without them)
-            LUFactor<F, N, double> ft;
+            // the register factor for small systems; thread-local memory from n = 6 on
+            using FT = typename std::conditional<(N >= 6), LocalLU<F, N>, LUFactor<F, N, double>>::type;
+            FT ft;
             ft.factor(fam, js);
             if (ft.info > 0) {
                 ok = false;

@@ -8,7 +8,7 @@ iterate bit for bit under the unfused arithmetic, which rounds like the CPU rest
 import numpy as np
 import pytest
 
-from workloads import c0, c1, cubic_affine, cubic_affine_pivoting
+from workloads import cubic_affine_illcond, c0, c1, cubic_affine, cubic_affine_pivoting
 
 pytestmark = pytest.mark.gpu
 
@@ -104,6 +104,23 @@ def test_mixed_fp32_refinement_parity(gsb, oracle, arith):
                                   opts)
     assert np.array_equal(sg["code"], s64["code"])
     assert np.all(rel_err(xg, x64) <= REL_TOL)
+
+
+@pytest.mark.parametrize("n", [4, 6, 8])
+def test_mixed_promotion(gsb, oracle, n):
+    # condition numbers 1e3..1e9: the Float32 factor needs its refinement passes and more than
+    # half of the systems are promoted to the Float64 factor (from n = 6 on, the thread-local
+    # one), with SUCCESS, MAXITERS, LINESEARCH_FAILED and STALLED among the outcomes
+    X0, P = cubic_affine_illcond(n, 8192, 5)
+    prob = gsb.NonlinearProblem(gsb.CubicAffine(n))
+    m = gsb.Newton(linsolve=gsb.LUFactorization("float32"), refinement=gsb.Refinement(),
+                   globalization=gsb.Backtracking(), arithmetic="unfused")
+    opts = gsb.Options(**OPTS)
+    xg, sg = run_gpu(gsb, prob, m, X0, P, opts)
+    xo, so = oracle.solve_batch(prob, m, X0.copy(), P, opts)
+    assert so["promoted"].sum() > X0.shape[0] // 3
+    assert len(np.unique(so["code"])) >= 3
+    check_parity(xg, sg, xo, so, bitwise=True)
 
 
 @pytest.mark.parametrize("n", [2, 4, 6])

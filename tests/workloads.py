@@ -44,3 +44,18 @@ def cubic_affine_pivoting(n, nsys, diag, config_id):
     b = np.take_along_axis(b, perm, axis=1)
     P = np.concatenate([A.transpose(0, 2, 1).reshape(nsys, n * n), b], axis=1)
     return X0, np.ascontiguousarray(P)
+
+
+def cubic_affine_illcond(n, nsys, config_id, log10_cond=(3.0, 9.0)):
+    """Cubic-affine systems whose A = Q1 diag(s) Q2 has a condition number drawn log-uniformly
+    from 10^log10_cond, so that the Float32 factor of the mixed form needs its refinement passes
+    and, on the ill-conditioned end, is promoted to Float64. b ~ 1e-3 U(-1, 1)^n, x0 = 0."""
+    g = rng(config_id, stream=11)
+    q1, _ = np.linalg.qr(g.standard_normal((nsys, n, n)))
+    q2, _ = np.linalg.qr(g.standard_normal((nsys, n, n)))
+    lc = g.uniform(log10_cond[0], log10_cond[1], nsys)
+    s = 10.0 ** (-lc[:, None] * np.linspace(0.0, 1.0, n)[None, :])
+    A = np.einsum("sij,sj,sjk->sik", q1, s, q2) * (n + 1.0)
+    b = g.uniform(-1.0, 1.0, (nsys, n)) * 1e-3
+    P = np.concatenate([A.transpose(0, 2, 1).reshape(nsys, n * n), b], axis=1)
+    return np.zeros((nsys, n)), np.ascontiguousarray(P)

@@ -7,6 +7,7 @@
 
 #include "../../include/gsb.h"
 #include "gsb_families.cuh"
+#include "gsb_lm.cuh"
 #include "gsb_newton.cuh"
 #include "gsb_numerics.cuh"
 #include "gsb_team.cuh"
@@ -197,6 +198,51 @@ __global__ void __launch_bounds__(kThreads) team_kernel(GsbMethod m, GsbOptions 
     }
 }
 
+// The least-squares form: one Levenberg–Marquardt solve per thread. Shared memory holds each
+// system's M observations (odd row stride) and, after the rows, the M abscissae of the batch.
+template <class Fam, bool F>
+__global__ void __launch_bounds__(kThreads, 3) lm_kernel(GsbMethod m, GsbOptions o, Launch L) {
+    extern __shared__ double smem[];
+    constexpr int N = Fam::N, M = Fam::M, RS = (M % 2 == 1) ? M : M + 1;
+    const int tid = threadIdx.x;
+    const int64_t base = (int64_t)blockIdx.x * blockDim.x;
+    const int64_t i = base + tid;
+    double* prow = smem + tid * RS;
+    double* tsh = smem + kThreads * RS;
+    for (int k = tid; k < M; k += blockDim.x) tsh[k] = __ldg(L.shared + k);
+    if (L.order == nullptr && L.p_layout == GSB_AOS) {
+        stage_aos<M, RS, kThreads>(smem, L.P + base * M, L.nsys - base, tid);
+    } else if (i < L.nsys) {
+        const int64_t idx = L.order ? L.order[i] - L.order_base : i;
+        if (L.p_layout == GSB_SOA) {
+#pragma unroll 4
+            for (int k = 0; k < M; ++k) prow[k] = __ldg(L.P + (int64_t)k * L.nsys + idx);
+        } else {
+#pragma unroll 4
+            for (int k = 0; k < M; ++k) prow[k] = __ldg(L.P + idx * M + k);
+        }
+    }
+    __syncthreads();
+    if (i >= L.nsys) return;
+    const int64_t idx = L.order ? L.order[i] - L.order_base : i;
+    Fam fam{prow, tsh};
+    double x[N];
+#pragma unroll
+    for (int k = 0; k < N; ++k)
+        x[k] = L.x_layout == GSB_SOA ? L.X[(int64_t)k * L.nsys + idx] : L.X[idx * N + k];
+    LMSolver<Fam, F> sv(fam, m, o);
+    double gr;
+    DevStatus s = sv.solve(x, gr);
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+        if (L.x_layout == GSB_SOA) L.X[(int64_t)k * L.nsys + idx] = x[k];
+        else L.X[idx * N + k] = x[k];
+    }
+    if (L.s_kind == GSB_STATUS64) store_status(L.S, idx, s, gr);
+    else reinterpret_cast<unsigned char*>(L.S)[idx] = (unsigned char)s.code;
+    if (L.tally) tally_code(L.tally, s.code);
+}
+
 using KernelFn = void (*)(GsbMethod, GsbOptions, Launch);
 
 struct KernelEntry {
@@ -209,6 +255,12 @@ struct KernelEntry {
 template <class Fam, bool F, bool Mixed, bool PlainRef> KernelEntry* entry() {
     static KernelEntry e{newton_kernel<Fam, F, Mixed, PlainRef>,
                          kThreads * row_stride(Fam::NP, Fam::N), kThreads, {}};
+    return &e;
+}
+
+template <class Fam, bool F> KernelEntry* lm_entry() {
+    constexpr int RS = (Fam::M % 2 == 1) ? Fam::M : Fam::M + 1;
+    static KernelEntry e{lm_kernel<Fam, F>, kThreads * RS + Fam::M, kThreads, {}};
     return &e;
 }
 

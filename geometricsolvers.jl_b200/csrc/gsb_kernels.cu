@@ -173,6 +173,7 @@ GSB_DECLARE_ENTRY(hetero6);
 GSB_DECLARE_ENTRY(coupled2);
 GSB_DECLARE_TEAM(cubic6);
 GSB_DECLARE_TEAM(cubic8);
+KernelEntry* lm_expsum3_64(bool fused);
 }  // namespace gsb
 
 namespace {
@@ -287,14 +288,32 @@ int launch_solve(const GsbProblem* prob, const GsbMethod* method, const GsbOptio
                  int32_t x_layout, void* S, int32_t s_kind, const double* P, int32_t p_layout,
                  const int64_t* order, int32_t order_base, int64_t nsys, cudaStream_t st,
                  unsigned long long* tally_dev) {
-    if (method->globalization == GSB_LEVENBERG_MARQUARDT)
-        return set_err(GSB_ERR_UNSUPPORTED, "LevenbergMarquardt batch kernel not in this build");
-    if (method->linsolve != GSB_LU)
-        return set_err(GSB_ERR_UNSUPPORTED, "QRFactorization batch kernel not in this build");
     const bool mixed = method->factor_precision == GSB_F32;
     const bool fused = method->arithmetic == GSB_FUSED;
-    KernelEntry* ke = select_kernel(prob, fused, mixed, method->refinement == GSB_REFINEMENT,
-                                    method->threads_per_system);
+    const bool lm = method->globalization == GSB_LEVENBERG_MARQUARDT;
+    KernelEntry* ke = nullptr;
+    if (prob->family == GSB_FAMILY_EXPSUM3_LSQ) {
+        // the least-squares family: the LevenbergMarquardt step on its stacked QR path
+        if (!lm)
+            return set_err(GSB_ERR_UNSUPPORTED,
+                           "the least-squares batch kernel runs the LevenbergMarquardt step");
+        if (mixed)
+            return set_err(GSB_ERR_UNSUPPORTED,
+                           "LevenbergMarquardt factors in the working precision");
+        if (method->threads_per_system > 1)
+            return set_err(GSB_ERR_UNSUPPORTED, "one thread per least-squares system");
+        if (prob->m != 64) return set_err(GSB_ERR_UNSUPPORTED, "no batch kernel for this m");
+        if (!prob->shared) return set_err(GSB_ERR_ARGUMENT, "the abscissae t are missing");
+        ke = lm_expsum3_64(fused);
+    } else {
+        if (lm)
+            return set_err(GSB_ERR_UNSUPPORTED,
+                           "LevenbergMarquardt batch kernel only for least-squares families");
+        if (method->linsolve != GSB_LU)
+            return set_err(GSB_ERR_UNSUPPORTED, "QRFactorization batch kernel not in this build");
+        ke = select_kernel(prob, fused, mixed, method->refinement == GSB_REFINEMENT,
+                           method->threads_per_system);
+    }
     if (!ke) return set_err(GSB_ERR_UNSUPPORTED, "no batch kernel for this family and size");
     int dev = 0;
     if (int rc = cuda_err(cudaGetDevice(&dev), "cudaGetDevice")) return rc;
@@ -413,14 +432,32 @@ int gsb_solve_batch(const GsbProblem* prob, const GsbMethod* method, const GsbOp
             seen[v] = 1;
         }
     }
-    if (method->globalization == GSB_LEVENBERG_MARQUARDT)
-        return set_err(GSB_ERR_UNSUPPORTED, "LevenbergMarquardt batch kernel not in this build");
-    if (method->linsolve != GSB_LU)
-        return set_err(GSB_ERR_UNSUPPORTED, "QRFactorization batch kernel not in this build");
     const bool mixed = method->factor_precision == GSB_F32;
     const bool fused = method->arithmetic == GSB_FUSED;
-    KernelEntry* ke = select_kernel(prob, fused, mixed, method->refinement == GSB_REFINEMENT,
-                                    method->threads_per_system);
+    const bool lm = method->globalization == GSB_LEVENBERG_MARQUARDT;
+    KernelEntry* ke = nullptr;
+    if (prob->family == GSB_FAMILY_EXPSUM3_LSQ) {
+        // the least-squares family: the LevenbergMarquardt step on its stacked QR path
+        if (!lm)
+            return set_err(GSB_ERR_UNSUPPORTED,
+                           "the least-squares batch kernel runs the LevenbergMarquardt step");
+        if (mixed)
+            return set_err(GSB_ERR_UNSUPPORTED,
+                           "LevenbergMarquardt factors in the working precision");
+        if (method->threads_per_system > 1)
+            return set_err(GSB_ERR_UNSUPPORTED, "one thread per least-squares system");
+        if (prob->m != 64) return set_err(GSB_ERR_UNSUPPORTED, "no batch kernel for this m");
+        if (!prob->shared) return set_err(GSB_ERR_ARGUMENT, "the abscissae t are missing");
+        ke = lm_expsum3_64(fused);
+    } else {
+        if (lm)
+            return set_err(GSB_ERR_UNSUPPORTED,
+                           "LevenbergMarquardt batch kernel only for least-squares families");
+        if (method->linsolve != GSB_LU)
+            return set_err(GSB_ERR_UNSUPPORTED, "QRFactorization batch kernel not in this build");
+        ke = select_kernel(prob, fused, mixed, method->refinement == GSB_REFINEMENT,
+                           method->threads_per_system);
+    }
     if (!ke) return set_err(GSB_ERR_UNSUPPORTED, "no batch kernel for this family and size");
     Workspace* ws = nullptr;
     if (tally) {

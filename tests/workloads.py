@@ -59,3 +59,18 @@ def cubic_affine_illcond(n, nsys, config_id, log10_cond=(3.0, 9.0)):
     b = g.uniform(-1.0, 1.0, (nsys, n)) * 1e-3
     P = np.concatenate([A.transpose(0, 2, 1).reshape(nsys, n * n), b], axis=1)
     return np.zeros((nsys, n)), np.ascontiguousarray(P)
+
+
+def c2(nsys=524288, m=64):
+    """Exp-sum least squares: t = linspace(0, 4, m) (shared), true a_j ~ U(0.5, 2) and b_j ~
+    U(0.1, 3) sorted ascending, y = sum_j a_j exp(-b_j t) + N(0, 1e-3^2), x0 = truth (1 + U(-0.2,
+    0.2)). x = (a1, b1, a2, b2, a3, b3). Returns (X0 (nsys, 6), Y (nsys, m), t (m,))."""
+    g = rng(2)
+    t = np.linspace(0.0, 4.0, m)
+    a = g.uniform(0.5, 2.0, (nsys, 3))
+    b = np.sort(g.uniform(0.1, 3.0, (nsys, 3)), axis=1)
+    y = np.einsum("sj,sji->si", a, np.exp(-b[:, :, None] * t[None, None, :]))
+    y += g.standard_normal((nsys, m)) * 1e-3
+    truth = np.stack([a[:, 0], b[:, 0], a[:, 1], b[:, 1], a[:, 2], b[:, 2]], axis=1)
+    X0 = truth * (1.0 + g.uniform(-0.2, 0.2, (nsys, 6)))
+    return np.ascontiguousarray(X0), np.ascontiguousarray(y), t

@@ -11,6 +11,7 @@
 #include "gsb_newton.cuh"
 #include "gsb_numerics.cuh"
 #include "gsb_team.cuh"
+#include "gsb_warp.cuh"
 
 namespace gsb {
 
@@ -243,6 +244,51 @@ __global__ void __launch_bounds__(kThreads, 3) lm_kernel(GsbMethod m, GsbOptions
     if (L.tally) tally_code(L.tally, s.code);
 }
 
+// The warp form (n = 12 ... 32): T lanes per system, kThreads / T systems per CTA. Each system's
+// shared memory holds its parameter block, then its N x LD factor.
+template <class Fam> __host__ __device__ constexpr int warp_sys_stride() {
+    return ((Fam::NP + 1) / 2) * 2 + Fam::N * warp_ld(Fam::N);
+}
+
+template <class Fam, int T, bool F, bool Mixed, bool PlainRef>
+__global__ void __launch_bounds__(kThreads) warp_kernel(GsbMethod m, GsbOptions o, Launch L) {
+    extern __shared__ double smem[];
+    constexpr int N = Fam::N, NP = Fam::NP, SPB = kThreads / T, SS = warp_sys_stride<Fam>();
+    const int tid = threadIdx.x;
+    const int team = tid / T;
+    const int64_t base = (int64_t)blockIdx.x * SPB;
+    const int64_t i = base + team;
+    double* sys = smem + team * SS;
+    if (L.order == nullptr && L.p_layout == GSB_AOS) {
+        stage_aos<NP, SS, SPB>(smem, L.P + base * NP, L.nsys - base, tid);
+    } else if (i < L.nsys) {
+        const int64_t idx = L.order ? L.order[i] - L.order_base : i;
+        for (int k = tid % T; k < NP; k += T)
+            sys[k] = L.p_layout == GSB_SOA ? __ldg(L.P + (int64_t)k * L.nsys + idx)
+                                           : __ldg(L.P + idx * NP + k);
+    }
+    __syncthreads();
+    if (i >= L.nsys) return;
+    const int64_t idx = L.order ? L.order[i] - L.order_base : i;
+    Team<T> tm;
+    const int lane = tm.lane;
+    Fam fam{sys};
+    double xl = 0.0;
+    if (lane < N) xl = L.x_layout == GSB_SOA ? L.X[(int64_t)lane * L.nsys + idx] : L.X[idx * N + lane];
+    WarpSolver<Fam, T, F, Mixed, PlainRef> sv(fam, m, o, tm, sys + ((NP + 1) / 2) * 2);
+    double gr;
+    DevStatus s = sv.solve(xl, gr);
+    if (lane < N) {
+        if (L.x_layout == GSB_SOA) L.X[(int64_t)lane * L.nsys + idx] = xl;
+        else L.X[idx * N + lane] = xl;
+    }
+    if (lane == 0) {
+        if (L.s_kind == GSB_STATUS64) store_status(L.S, idx, s, gr);
+        else reinterpret_cast<unsigned char*>(L.S)[idx] = (unsigned char)s.code;
+        if (L.tally) tally_code(L.tally, s.code);
+    }
+}
+
 using KernelFn = void (*)(GsbMethod, GsbOptions, Launch);
 
 struct KernelEntry {
@@ -262,6 +308,22 @@ template <class Fam, bool F> KernelEntry* lm_entry() {
     constexpr int RS = (Fam::M % 2 == 1) ? Fam::M : Fam::M + 1;
     static KernelEntry e{lm_kernel<Fam, F>, kThreads * RS + Fam::M, kThreads, {}};
     return &e;
+}
+
+template <class Fam, int T, bool F, bool Mixed, bool PlainRef> KernelEntry* warp_entry() {
+    static KernelEntry e{warp_kernel<Fam, T, F, Mixed, PlainRef>,
+                         (kThreads / T) * warp_sys_stride<Fam>(), kThreads / T, {}};
+    return &e;
+}
+
+// The six warp-form kernels of a family at team size T.
+template <class Fam, int T> KernelEntry* pick_warp(bool fused, bool mixed, bool refine) {
+    if (fused) {
+        if (mixed) return warp_entry<Fam, T, true, true, false>();
+        return refine ? warp_entry<Fam, T, true, false, true>() : warp_entry<Fam, T, true, false, false>();
+    }
+    if (mixed) return warp_entry<Fam, T, false, true, false>();
+    return refine ? warp_entry<Fam, T, false, false, true>() : warp_entry<Fam, T, false, false, false>();
 }
 
 template <class Fam, int T, bool Mixed> KernelEntry* team_entry() {

@@ -174,6 +174,10 @@ GSB_DECLARE_ENTRY(coupled2);
 GSB_DECLARE_TEAM(cubic6);
 GSB_DECLARE_TEAM(cubic8);
 KernelEntry* lm_expsum3_64(bool fused);
+KernelEntry* warp_cubic12(bool fused, bool mixed, bool refine);
+KernelEntry* warp_cubic16(bool fused, bool mixed, bool refine);
+KernelEntry* warp_cubic24(bool fused, bool mixed, bool refine);
+KernelEntry* warp_cubic32(bool fused, bool mixed, bool refine);
 }  // namespace gsb
 
 namespace {
@@ -190,6 +194,18 @@ int tuned_team(const GsbProblem* prob, bool mixed) {
 
 // The kernel of a call: the one-thread solve for T = 1, else the team solve (fused only).
 KernelEntry* select_kernel(const GsbProblem* prob, bool fused, bool mixed, bool refine, int T) {
+    if (prob->family == GSB_FAMILY_CUBIC_AFFINE && prob->n >= 12) {
+        // the warp form: 16 lanes per system up to n = 16, a whole warp above
+        const int tw = prob->n <= 16 ? 16 : 32;
+        if (T != 0 && T != tw) return nullptr;
+        switch (prob->n) {
+        case 12: return warp_cubic12(fused, mixed, refine);
+        case 16: return warp_cubic16(fused, mixed, refine);
+        case 24: return warp_cubic24(fused, mixed, refine);
+        case 32: return warp_cubic32(fused, mixed, refine);
+        default: return nullptr;
+        }
+    }
     if (T == 0) T = fused ? tuned_team(prob, mixed) : 1;
     if (T != 1) {
         if (!fused || prob->family != GSB_FAMILY_CUBIC_AFFINE) return nullptr;

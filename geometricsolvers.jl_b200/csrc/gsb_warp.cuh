@@ -1,0 +1,709 @@
+// The warp form of the per-system Newton solve, for systems too large for one thread's
+// registers (n = 12 ... 32): a team of T = 16 or 32 lanes (an aligned part of a warp) runs one
+// system. Lane i < n owns component i of every vector (iterate, residual, direction, trial) and
+// row i of the Jacobian's factor; the factor lives in shared memory, so the column loop of the
+// elimination and the row exchanges of partial pivoting take runtime indices.
+//
+// Every operation is the one-thread solve's (gsb_newton.cuh) in the same order: the LU of
+// src/linear/static/lu.jl:24-92 (first largest pivot, info = first zero pivot), the scalings of
+// factor_matrix and ldiv!! (src/linear/factors.jl:802-949), the left-fold norms and products of
+// src/base/reductions.jl, Backtracking and Static (src/globalization/linefunction.jl:114-199,
+// backtracking.jl:62-132), refinement (src/nonlinear/refinement.jl:211-244) and the mixed
+// step's promotion (src/nonlinear/newton.jl:1604-1720). A fold over a distributed vector
+// broadcasts its entries in index order, so each lane computes the same left fold bit for bit
+// and the control flow of a team stays uniform; under unfused arithmetic the results equal the
+// oracle's exactly, as the one-thread kernels' do.
+#pragma once
+
+#include "../../include/gsb.h"
+#include "gsb_families.cuh"
+#include "gsb_newton.cuh"
+#include "gsb_numerics.cuh"
+#include "gsb_team.cuh"
+
+namespace gsb {
+
+// Leading dimension of a factor row in shared memory: odd, so that the lanes' rows fall in
+// distinct 8-byte bank slots.
+__host__ __device__ constexpr int warp_ld(int n) { return (n % 2 == 1) ? n : n + 1; }
+
+// The cubic-affine family in row form: F_i(x) = (A x)_i + 0.1 x_i^3 - b_i with the one-thread
+// family's operations (gsb_families.cuh). `p` is the system's parameter block in shared memory
+// (A column-major, then b).
+template <int N_> struct WarpCubic {
+    static constexpr int N = N_, NP = N_ * N_ + N_;
+    const double* p;
+    __device__ __forceinline__ double par(int k) const { return lds(smem_addr(p) + 8u * k); }
+    __device__ __forceinline__ double A(int i, int k) const { return par(i + k * N); }
+
+    // Row i (< N) of F; every lane of the team calls it (x_j arrive by broadcast).
+    template <int T>
+    __device__ __forceinline__ double F(const Team<T>& tm, int i, double xl) const {
+        const int r = i < N ? i : N - 1;
+        double t = __dmul_rn(A(r, 0), tm.bcast(xl, 0));
+#pragma unroll 8
+        for (int j = 1; j < N; ++j) t = __fma_rn(A(r, j), tm.bcast(xl, j), t);
+        const double c = __dmul_rn(__dmul_rn(xl, xl), xl);
+        return __dsub_rn(__fma_rn(0.1, c, t), par(N * N + r));
+    }
+    // The diagonal of J at x (the rest of J is A).
+    __device__ __forceinline__ double diag(int i, double xi) const {
+        const int r = i < N ? i : N - 1;
+        const double cp = __dadd_rn(__dmul_rn(__dadd_rn(xi, xi), xi), __dmul_rn(xi, xi));
+        return __fma_rn(0.1, cp, A(r, r));
+    }
+    __device__ __forceinline__ double J(int i, int k, double diag_i) const {
+        return i == k ? diag_i : A(i, k);
+    }
+    template <int T>
+    __device__ __forceinline__ double jvp(const Team<T>& tm, int i, double xi, double vl) const {
+        const int r = i < N ? i : N - 1;
+        double t = __dmul_rn(A(r, 0), tm.bcast(vl, 0));
+#pragma unroll 8
+        for (int j = 1; j < N; ++j) t = __fma_rn(A(r, j), tm.bcast(vl, j), t);
+        const double xv = __dmul_rn(vl, xi);
+        const double x2p = __dadd_rn(xv, xv);
+        const double cp = __dadd_rn(__dmul_rn(x2p, xi), __dmul_rn(vl, __dmul_rn(xi, xi)));
+        return __fma_rn(0.1, cp, t);
+    }
+};
+
+// Ordered folds over a vector distributed one entry per lane (lanes >= N hold padding).
+template <int N, int T, bool F> struct WarpVec {
+    using A = Arith<F>;
+    const Team<T>& tm;
+    __device__ WarpVec(const Team<T>& t) : tm(t) {}
+
+    __device__ __forceinline__ double norm2(double v) const {
+        const double v0 = tm.bcast(v, 0);
+        double s = A::mul(v0, v0);
+#pragma unroll 8
+        for (int i = 1; i < N; ++i) {
+            const double vi = tm.bcast(v, i);
+            s = A::madd(vi, vi, s);
+        }
+        return s;
+    }
+    __device__ __forceinline__ double dot(double a, double b) const {
+        double s = A::mul(tm.bcast(a, 0), tm.bcast(b, 0));
+#pragma unroll 8
+        for (int i = 1; i < N; ++i) s = A::madd(tm.bcast(a, i), tm.bcast(b, i), s);
+        return s;
+    }
+    __device__ __forceinline__ double maxabs(double v) const {
+        double m = fabs(tm.bcast(v, 0));
+#pragma unroll 8
+        for (int i = 1; i < N; ++i) m = jmax(m, fabs(tm.bcast(v, i)));
+        return m;
+    }
+    // rnorm_from: the norm from its norm2 s, with the scaled fallback.
+    __device__ double rnorm_from(double v, double s) const {
+        if (isfin(s) && s >= double(N) * kFloatmin) return sqrt(s);
+        double m = jmax(fabs(tm.bcast(v, 0)), 0.0);
+        for (int i = 1; i < N; ++i) m = jmax(m, jmax(fabs(tm.bcast(v, i)), 0.0));
+        if (m == 0.0 || !isfin(m)) return m;
+        const int e = jexponent(m);
+        const double t = ldexp2_slow(tm.bcast(v, 0), -e);
+        double acc = A::mul(t, t);
+        for (int i = 1; i < N; ++i) {
+            const double u = ldexp2_slow(tm.bcast(v, i), -e);
+            acc = A::madd(u, u, acc);
+        }
+        return ldexp2_slow(sqrt(acc), e);
+    }
+    __device__ __forceinline__ double rnorm(double v) const { return rnorm_from(v, norm2(v)); }
+    // matrix_exponent over the entries of the vector (factors.jl:833-843)
+    __device__ __forceinline__ int exponent(double v, bool mine) const {
+        unsigned long long b = mine ? (FBits<double>::bits(v) & ~FBits<double>::sign_mask) : 0ull;
+        const double m = FBits<double>::from(tm.umax(b));
+        if (!(isfin(m) && m != 0.0)) return 0;
+        const int e = jexponent(m);
+        return e > 1023 ? 1023 : (e < -1023 ? -1023 : e);
+    }
+};
+
+// The pivoted LU of an N x N matrix in shared memory, rows at a + i * LD; lane k keeps the
+// pivot of column k in `piv`.
+template <int N, int T, bool F, class TF> struct WarpLU {
+    static constexpr int LD = warp_ld(N);
+    using A = Arith<F>;
+    TF* a;
+    int piv;
+    int info, e;
+
+    __device__ __forceinline__ TF& at(int i, int j) const { return a[i * LD + j]; }
+
+    // J into the factor (row `lane` from the lane's row values), factor_matrix's scaling, then
+    // the elimination (lu.jl:24-64).
+    template <class Fam>
+    __device__ void factor(const Team<T>& tm, const Fam& fam, double diag_i) {
+        const int lane = tm.lane;
+        const bool mine = lane < N;
+        constexpr bool same = sizeof(TF) == sizeof(double);
+        unsigned long long mb = 0ull;
+        if (mine)
+            for (int k = 0; k < N; ++k) {
+                const unsigned long long b =
+                    FBits<double>::bits(fam.J(lane, k, diag_i)) & ~FBits<double>::sign_mask;
+                mb = b > mb ? b : mb;
+            }
+        const double mm = FBits<double>::from(tm.umax(mb));
+        if constexpr (same) {
+            int ex = 0;
+            if (isfin(mm) && mm != 0.0) {
+                ex = jexponent(mm);
+                ex = ex > 1023 ? 1023 : (ex < -1023 ? -1023 : ex);
+            }
+            e = ex < 0 ? ex : 0;
+            if (mine)
+                for (int k = 0; k < N; ++k) {
+                    const double v = fam.J(lane, k, diag_i);
+                    at(lane, k) = e < 0 ? scale2_in(v, -e) : v;  // -e in [1, 1023]
+                }
+        } else {
+            e = (isfin(mm) && mm != 0.0) ? max(-1023, min(1023, jexponent(mm))) : 0;
+            if (mine)
+                for (int k = 0; k < N; ++k) {
+                    const double v = fam.J(lane, k, diag_i);
+                    at(lane, k) = TF(e == 0 ? v : scale2_in(v, -e));  // -e in [-1023, 1023]
+                }
+        }
+        __syncwarp(tm.mask);
+        info = 0;
+        piv = lane;
+        for (int k = 0; k < N; ++k) {
+            // the first largest |a_ik|, i >= k (a NaN on the diagonal keeps k; a NaN below it
+            // never wins), as a (value, index) maximum with the smaller index on ties
+            double w = -2.0;
+            if (lane == k) {
+                const double v = double(fabs(at(k, k)));
+                w = v != v ? kInf : v;
+            } else if (lane > k && lane < N) {
+                const double v = double(fabs(at(lane, k)));
+                w = v != v ? -1.0 : v;
+            }
+            int wi = lane;
+#pragma unroll
+            for (int off = T / 2; off > 0; off >>= 1) {
+                const double ow = __shfl_xor_sync(tm.mask, w, off, T);
+                const int oi = __shfl_xor_sync(tm.mask, wi, off, T);
+                if (ow > w || (ow == w && oi < wi)) {
+                    w = ow;
+                    wi = oi;
+                }
+            }
+            const int p = wi;
+            if (lane == k) piv = p;
+            if (p != k) {
+                if (mine) {
+                    const TF t = at(k, lane);
+                    at(k, lane) = at(p, lane);
+                    at(p, lane) = t;
+                }
+                __syncwarp(tm.mask);
+            }
+            const TF akk = at(k, k);
+            if (akk == TF(0)) {
+                if (info == 0) info = k + 1;
+            } else if (lane > k && lane < N) {
+                const TF l = at(lane, k) / akk;
+                at(lane, k) = l;
+                for (int j = k + 1; j < N; ++j) at(lane, j) = A::msub(l, at(k, j), at(lane, j));
+            }
+            __syncwarp(tm.mask);
+        }
+    }
+
+    // lu.jl:67-92 on the distributed right-hand side x.
+    __device__ void backsolve(const Team<T>& tm, TF& x) const {
+        const int lane = tm.lane;
+        for (int k = 0; k < N; ++k) {
+            const int p = tm.bcast(piv, k);
+            if (p != k) {
+                const TF xk = tm.bcast(x, k);
+                const TF xp = tm.bcast(x, p);
+                if (lane == k) x = xp;
+                else if (lane == p) x = xk;
+            }
+        }
+        for (int k = 0; k < N; ++k) {
+            const TF xk = tm.bcast(x, k);
+            if (lane > k && lane < N) x = A::msub(at(lane, k), xk, x);
+        }
+        for (int k = N - 1; k >= 0; --k) {
+            if (lane == k) x = x / at(k, k);
+            const TF xk = tm.bcast(x, k);
+            if (lane < k) x = A::msub(at(lane, k), xk, x);
+        }
+    }
+
+    // ldiv!!: same type (factors.jl:931-936) or mixed type (factors.jl:943-949).
+    __device__ double ldiv(const Team<T>& tm, const WarpVec<N, T, F>& wv, double r) const {
+        const bool mine = tm.lane < N;
+        if constexpr (sizeof(TF) == sizeof(double)) {
+            // rhs_exponent (factors.jl:880-885)
+            const int m = wv.exponent(r, mine);
+            const int lo = e < 0 ? e : 0;
+            const int aa = m > 0 ? 0 : (m < lo ? lo : m);
+            const int bb = m - (1023 - headroom(N));
+            const int k = aa > bb ? aa : bb;
+            TF x = k == 0 ? r : scale2_in(r, -k);  // -k in [-6, 1023]
+            backsolve(tm, x);
+            const int e2 = k - e;
+            return e2 == 0 ? double(x) : scale2_in(double(x), e2);  // e2 in [0, 1029]
+        } else {
+            const double s = wv.maxabs(r);
+            if (s == 0.0) return 0.0;
+            TF x = TF(__ddiv_rn(r, s));
+            backsolve(tm, x);
+            int ex = 0;
+            double frac = isfin(s) ? frexp(s, &ex) : s;
+            if (!isfin(s)) ex = 0;
+            double d = __dmul_rn(double(x), frac);
+            const int E = ex - e;
+            return (E >= -1074 && E <= 2046) ? scale2_in(d, E) : ldexp2_slow(d, E);
+        }
+    }
+};
+
+template <class Fam, int T, bool F, bool Mixed, bool PlainRef> struct WarpSolver {
+    static constexpr int N = Fam::N, LD = warp_ld(N);
+    using A = Arith<F>;
+    const Fam& fam;
+    const GsbMethod& m;
+    const GsbOptions& o;
+    const Team<T>& tm;
+    double* lu;  // N x LD doubles of shared memory for the factor (a Float32 factor uses half)
+    WarpVec<N, T, F> wv;
+
+    __device__ WarpSolver(const Fam& f, const GsbMethod& mm, const GsbOptions& oo,
+                          const Team<T>& t, double* l)
+        : fam(f), m(mm), o(oo), tm(t), lu(l), wv(t) {}
+
+    __device__ __forceinline__ bool has_merit() const { return m.globalization == GSB_BACKTRACKING; }
+    __device__ __forceinline__ double Fr(double xl) const { return fam.template F<T>(tm, tm.lane, xl); }
+
+    // J v with the held Jacobian, row `lane`, as a left fold over the columns.
+    __device__ __forceinline__ double jmul(double diag_i, double vl) const {
+        const int i = tm.lane < N ? tm.lane : N - 1;
+        double s = A::mul(fam.J(i, 0, diag_i), tm.bcast(vl, 0));
+        for (int k = 1; k < N; ++k) s = A::madd(fam.J(i, k, diag_i), tm.bcast(vl, k), s);
+        return s;
+    }
+
+    // grad_ratio_and_norm, src/nonlinear/newton.jl:1287-1298.
+    __device__ void grad_ratio_and_norm(double diag_i, double Fl, double fnorm, double& gr,
+                                        double& jnorm) const {
+        // ‖J‖_F as the column-major left fold: every lane folds all entries (the diagonal
+        // arrives by broadcast, the rest is A)
+        double s = 0.0, mx = 0.0;
+        for (int k = 0; k < N; ++k) {
+            const double dk = tm.bcast(diag_i, k);
+            for (int i = 0; i < N; ++i) {
+                const double v = i == k ? dk : fam.A(i, k);
+                s = (i == 0 && k == 0) ? A::mul(v, v) : A::madd(v, v, s);
+                mx = (i == 0 && k == 0) ? jmax(fabs(v), 0.0) : jmax(mx, jmax(fabs(v), 0.0));
+            }
+        }
+        if (isfin(s) && s >= double(N * N) * kFloatmin) {
+            jnorm = sqrt(s);
+        } else if (mx == 0.0 || !isfin(mx)) {
+            jnorm = mx;
+        } else {
+            const int e = jexponent(mx);
+            double acc = 0.0;
+            for (int k = 0; k < N; ++k) {
+                const double dk = tm.bcast(diag_i, k);
+                for (int i = 0; i < N; ++i) {
+                    const double u = scale2_in(i == k ? dk : fam.A(i, k), -e);
+                    acc = (i == 0 && k == 0) ? A::mul(u, u) : A::madd(u, u, acc);
+                }
+            }
+            jnorm = scale2_in(sqrt(acc), e);
+        }
+        if (jnorm == 0.0 || fnorm == 0.0) {
+            gr = 0.0;
+            return;
+        }
+        // g_j = sum_i J_ij F_i: lane j folds column j
+        const int j = tm.lane < N ? tm.lane : N - 1;
+        const double dj = diag_i;
+        double g = A::mul(fam.J(0, j, tm.bcast(dj, 0)), tm.bcast(Fl, 0));
+        for (int i = 1; i < N; ++i) g = A::madd(i == j ? dj : fam.A(i, j), tm.bcast(Fl, i), g);
+        const double gnorm = wv.rnorm(g);
+        if (isfin(gnorm) || !(isfin(jnorm) && isfin(fnorm))) {
+            gr = __ddiv_rn(__ddiv_rn(gnorm, jnorm), fnorm);
+            return;
+        }
+        const int e = jexponent(fnorm);
+        const double sc = ldexp(1.0, -e);
+        g = A::mul(fam.J(0, j, tm.bcast(dj, 0)), __dmul_rn(tm.bcast(Fl, 0), sc));
+        for (int i = 1; i < N; ++i)
+            g = A::madd(i == j ? dj : fam.A(i, j), __dmul_rn(tm.bcast(Fl, i), sc), g);
+        gr = __ddiv_rn(__ddiv_rn(wv.rnorm(g), jnorm), ldexp(fnorm, -e));
+    }
+
+    __device__ __forceinline__ double residual_norm(const DevState& st, double Fl) const {
+        if (has_merit()) {
+            if (isfin(st.merit) && st.merit >= double(N) * kFloatmin) return sqrt(st.merit);
+            return wv.rnorm(Fl);
+        }
+        return isnan(st.fnorm) ? wv.rnorm(Fl) : st.fnorm;
+    }
+
+    // The merit of x + a d: the lane's trial entries and norm2 of the trial residual.
+    __device__ __forceinline__ double trial(double xl, double dl, double a, double& xt,
+                                            double& Ft) const {
+        xt = A::madd(a, dl, xl);
+        Ft = Fr(xt);
+        return wv.norm2(Ft);
+    }
+
+    __device__ __forceinline__ double slope0(double xl, double dl) const {
+        const double x0 = A::madd(0.0, dl, xl);
+        const double F0 = Fr(x0);
+        const double Jv = fam.template jvp<T>(tm, tm.lane, x0, dl);
+        return 2.0 * wv.dot(F0, Jv);
+    }
+
+    __device__ void globalize(double& xl, double& Fl, double dl, bool exact, double& merit,
+                              StepInfo& info) const {
+        if (m.globalization == GSB_STATIC) {
+            const double s = m.static_alpha;
+            const double dn = wv.rnorm(dl);
+            const double stepnorm = __dmul_rn(fabs(s), dn);
+            if (!isfin(stepnorm)) {
+                info = {NONFINITE, wv.rnorm(Fl), stepnorm, 0, false, false, false};
+                return;
+            }
+            double xp, Fp;
+            const double fn = wv.rnorm_from(Fp, trial(xl, dl, s, xp, Fp));
+            if (!isfin(fn)) {
+                info = {NONFINITE, wv.rnorm(Fl), stepnorm, 0, false, false, false};
+                return;
+            }
+            xl = xp;
+            Fl = Fp;
+            info = {SUCCESS, fn, stepnorm, 0, false, false, false};
+            return;
+        }
+        const double phi0 = merit;
+        const double dn = wv.rnorm(dl);
+        if (!isfin(dn)) {
+            info = {NONFINITE, wv.rnorm(Fl), dn, 0, false, false, false};
+            return;
+        }
+        double alpha = 1.0;
+        const double d0 = exact ? -2.0 * phi0 : slope0(xl, dl);
+        int code;
+        double aa = alpha, pa = kNaN;
+        double xt = xl, Ft = Fl;
+        if (!(isfin(phi0) && isfin(d0) && d0 < 0.0)) {
+            code = (isfin(phi0) && isfin(d0)) ? (d0 > 0.0 ? LINESEARCH_FAILED : STALLED) : NONFINITE;
+        } else {
+            const double tau = jmax(__dmul_rn(4.0 * kEps, fabs(phi0)), 4.0 * 4.9406564584124654e-324);
+            const double amin = jmax(__ddiv_rn(tau, fabs(d0)), kFloatmin);
+            alpha = jmin(jmax(alpha, amin), kInf);
+            double ap = kNaN, pp = kNaN;
+            int frozen = 0, trips = 0;
+            code = LINESEARCH_FAILED;
+            bool done = false;
+            const double c1 = m.bt_c1, p = m.bt_p;
+            while (!done && trips < m.bt_maxiter) {
+                ++trips;
+                aa = alpha;
+                pa = trial(xl, dl, alpha, xt, Ft);
+                frozen = (pa == phi0 && alpha <= kSqrtEps) ? frozen + 1 : 0;
+                const double demand = __dmul_rn(__dmul_rn(c1, alpha), d0);
+                if (__dsub_rn(pa, phi0) <= jmin(0.0, __dadd_rn(demand, tau))) {
+                    if (isfin(pa) && __dsub_rn(pa, phi0) < -tau) code = SUCCESS;
+                    else code = fabs(__dsub_rn(pa, phi0)) <= tau ? STALLED : LINESEARCH_FAILED;
+                    done = true;
+                } else if (frozen >= 2) {
+                    code = STALLED;
+                    done = true;
+                } else if (alpha <= amin) {
+                    code = fabs(__dsub_rn(pa, phi0)) <= tau ? STALLED : LINESEARCH_FAILED;
+                    done = true;
+                } else {
+                    double an;
+                    if (isfin(pa)) {
+                        an = kNaN;
+                        const double s = fabs(d0);
+                        const double r1 = __dadd_rn(__ddiv_rn(__dsub_rn(pa, phi0), s), alpha);
+                        if (!(ap > 0.0)) {
+                            if (r1 > 0.0) an = __ddiv_rn(__dmul_rn(alpha, alpha), __dmul_rn(2.0, r1));
+                        } else if (isfin(pp) && alpha != ap) {
+                            const double q1 = __ddiv_rn(r1, __dmul_rn(alpha, alpha));
+                            const double q2 = __ddiv_rn(__dadd_rn(__ddiv_rn(__dsub_rn(pp, phi0), s), ap),
+                                                        __dmul_rn(ap, ap));
+                            const double da = __dsub_rn(alpha, ap);
+                            const double Aq = __ddiv_rn(__dsub_rn(q1, q2), da);
+                            const double Bq =
+                                __ddiv_rn(__dsub_rn(__dmul_rn(alpha, q2), __dmul_rn(ap, q1)), da);
+                            const double disc = __dadd_rn(__dmul_rn(Bq, Bq), __dmul_rn(3.0, Aq));
+                            if (disc >= 0.0)
+                                an = Bq > 0.0 ? __ddiv_rn(1.0, __dadd_rn(Bq, sqrt(disc)))
+                                              : __ddiv_rn(__dadd_rn(-Bq, sqrt(disc)), __dmul_rn(3.0, Aq));
+                        }
+                        if (!(isfin(an) && an > 0.0)) an = __dmul_rn(p, alpha);
+                        an = jmin(jmax(an, __dmul_rn(0.1, alpha)), __dmul_rn(p, alpha));
+                    } else {
+                        an = jmin(__dmul_rn(0.1, alpha), __dmul_rn(sqrt(alpha), sqrt(amin)));
+                    }
+                    ap = alpha;
+                    pp = pa;
+                    alpha = jmax(an, amin);
+                }
+            }
+        }
+        if (code == SUCCESS) {
+            xl = xt;
+            Fl = Ft;
+            info = {SUCCESS, sqrt(pa), __dmul_rn(aa, dn), 0, false, false, aa < 1.0};
+            merit = pa;
+        } else if (code == LINESEARCH_FAILED) {
+            if (isfin(pa) && pa < phi0) {
+                xl = xt;
+                Fl = Ft;
+                info = {LINESEARCH_FAILED, sqrt(pa), __dmul_rn(aa, dn), 1, false, false, aa < 1.0};
+                merit = pa;
+            } else {
+                info = {LINESEARCH_FAILED, wv.rnorm(Fl), 0.0, 1, false, false, false};
+            }
+        } else if (code == STALLED) {
+            info = {STALLED, wv.rnorm(Fl), 0.0, 0, false, false, false};
+        } else {
+            info = {NONFINITE, wv.rnorm(Fl), 0.0, 0, false, false, false};
+        }
+    }
+
+    // refine_passes!! with the held Jacobian (refinement.jl:211-244); returns `failed`.
+    template <class Fac>
+    __device__ bool refine(double& dl, const Fac& fac, double diag_i, double Fl) const {
+        const double fnorm = wv.rnorm(Fl);
+        if (fnorm == 0.0) return false;
+        if (!isfin(fnorm)) return true;
+        const double thr = __dmul_rn(jmax(m.refine_eta, kSqrtEps), fnorm);
+        double r = jmul(diag_i, dl);
+        r = __dadd_rn(-Fl, -r);
+        double rprev = wv.rnorm(r);
+        if (!isfin(rprev)) return true;
+        if (rprev <= thr) return false;
+        for (int it = 1; it <= m.refine_maxiter; ++it) {
+            double dc = fac.ldiv(tm, wv, r);
+            dc = __dadd_rn(dl, dc);
+            r = jmul(diag_i, dc);
+            r = __dadd_rn(-Fl, -r);
+            const double rc = wv.rnorm(r);
+            if (!(rc < rprev)) return true;
+            dl = dc;
+            rprev = rc;
+            if (rc <= thr) return false;
+        }
+        return true;
+    }
+
+    __device__ void step_plain(DevState& st, double& xl, double& Fl, StepInfo& info) const {
+        const double fnorm = residual_norm(st, Fl);
+        const double diag_i = fam.diag(tm.lane, xl);
+        double gr, jn;
+        grad_ratio_and_norm(diag_i, Fl, fnorm, gr, jn);
+        double merit = st.merit;
+        WarpLU<N, T, F, double> fac{lu};
+        fac.factor(tm, fam, diag_i);
+        if (fac.info > 0) {
+            info = {SINGULAR, wv.rnorm(Fl), 0.0, 0, false, false, false};
+        } else {
+            double dl = -fac.ldiv(tm, wv, Fl);
+            if constexpr (PlainRef) refine(dl, fac, diag_i, Fl);
+            globalize(xl, Fl, dl, !PlainRef, merit, info);
+        }
+        st.gradratio = gr;
+        st.jnorm = jn;
+        st.merit = merit;
+        st.fnorm = info.fnorm;
+    }
+
+    __device__ void step_mixed(DevState& st, double& xl, double& Fl, StepInfo& info) const {
+        const double fnorm_old = residual_norm(st, Fl);
+        const bool was_promoted = st.promoted;
+        const double diag_i = fam.diag(tm.lane, xl);
+        double gr, jn;
+        grad_ratio_and_norm(diag_i, Fl, fnorm_old, gr, jn);
+        st.gradratio = gr;
+        st.jnorm = jn;
+        const bool ref = m.refinement == GSB_REFINEMENT;
+        double dl = 0.0;
+        bool ok = true;
+        int failures = 0;
+        double lin_rel = 0.0;
+        bool md_promoted = was_promoted;
+        bool fallback = was_promoted;
+        if (!was_promoted) {
+            WarpLU<N, T, F, float> fac{reinterpret_cast<float*>(lu)};
+            fac.factor(tm, fam, diag_i);
+            bool ref_failed;
+            if (fac.info > 0) {
+                ref_failed = true;
+            } else {
+                dl = -fac.ldiv(tm, wv, Fl);
+                ref_failed = ref ? refine(dl, fac, diag_i, Fl) : false;
+            }
+            if (ref_failed || fac.info > 0) {
+                failures += 1;
+                md_promoted = true;
+                fallback = true;
+            } else if (fnorm_old == 0.0 || !isfin(fnorm_old)) {
+                lin_rel = 0.0;
+            } else {
+                const double lin = __dadd_rn(Fl, jmul(diag_i, dl));
+                lin_rel = __ddiv_rn(wv.rnorm(lin), fnorm_old);
+            }
+        }
+        if (fallback) {
+            WarpLU<N, T, F, double> ft{lu};
+            ft.factor(tm, fam, diag_i);
+            if (ft.info > 0) {
+                ok = false;
+            } else {
+                dl = -ft.ldiv(tm, wv, Fl);
+                if (was_promoted && ref) refine(dl, ft, diag_i, Fl);
+            }
+        }
+        if (!ok) {
+            st.promoted = md_promoted;
+            info = {SINGULAR, wv.rnorm(Fl), 0.0, failures, md_promoted, false, false};
+            return;
+        }
+        const bool promoted_step = md_promoted && !was_promoted;
+        const bool exact_step = md_promoted;
+        double merit = st.merit;
+        globalize(xl, Fl, dl, exact_step, merit, info);
+        info.failures += failures;
+        if (promoted_step) {
+            info.promoted = true;
+            st.promoted = true;
+            st.slow_steps = 0;
+        } else if (!was_promoted) {
+            const double eta_lin = 1e-4;
+            if (info.fnorm > __dmul_rn(0.5, fnorm_old) && lin_rel > eta_lin) {
+                const int slow = st.slow_steps + 1;
+                if (slow >= 2) {
+                    st.promoted = true;
+                    st.slow_steps = 0;
+                    info.failures += 1;
+                    info.promoted = true;
+                } else {
+                    st.promoted = false;
+                    st.slow_steps = slow;
+                }
+            } else {
+                st.promoted = false;
+                st.slow_steps = 0;
+            }
+        }
+        st.merit = merit;
+        st.fnorm = info.fnorm;
+    }
+
+    __device__ __forceinline__ bool residual_converged(const DevStatus& s, double ft,
+                                                       double ft0) const {
+        if (!(s.iterations >= o.min_iterations)) return false;
+        return ft <= jmax(o.f_abstol, __dmul_rn(o.f_reltol, ft0));
+    }
+
+    // solve!!, src/nonlinear/solver.jl:277-378; the lane's entry of x in `xl`.
+    __device__ DevStatus solve(double& xl, double& gr_out) const {
+        double Fl = Fr(xl);
+        const double n2 = wv.norm2(Fl);
+        const double fnorm0 = wv.rnorm_from(Fl, n2);
+        DevState st;
+        st.merit = has_merit() ? n2 : kNaN;
+        st.fnorm = fnorm0;
+        st.gradratio = kNaN;
+        st.jnorm = 0.0;
+        st.promoted = false;
+        st.slow_steps = 0;
+        DevStatus s;
+        s.code = SUCCESS;
+        s.iterations = 0;
+        s.fnorm = fnorm0;
+        s.stepnorm = 0.0;
+        s.step_failures = 0;
+        s.promoted = false;
+        s.stationary = false;
+        s.rate = kNaN;
+        s.contracted = false;
+        gr_out = kNaN;
+        if (!isfin(fnorm0)) {
+            s.code = NONFINITE;
+            return s;
+        }
+        const double ftest0 = o.norm == 1 ? wv.maxabs(Fl) : fnorm0;
+        if (residual_converged(s, ftest0, ftest0)) return s;
+        if (o.max_iterations == 0) {
+            s.code = MAXITERS;
+            return s;
+        }
+        int stalls = 0;
+        while (true) {
+            const double rate_k = s.rate;
+            StepInfo info;
+            if (Mixed) step_mixed(st, xl, Fl, info);
+            else step_plain(st, xl, Fl, info);
+            record(s, info);
+            gr_out = st.gradratio;
+            if (info.code == SINGULAR || info.code == NONFINITE || info.code == MAXITERS) return s;
+            if (info.code == LINESEARCH_FAILED && info.stepnorm == 0.0) return s;
+            const double ft = o.norm == 1 ? wv.maxabs(Fl) : s.fnorm;
+            if (residual_converged(s, ft, ftest0)) {
+                s.code = SUCCESS;
+                s.stationary = false;
+                s.contracted = false;
+                return s;
+            }
+            const bool steptested = !(info.code == STALLED || info.limited);
+            const double xnorm = steptested ? wv.rnorm(xl) : kNaN;
+            bool contracted = false;
+            if (!info.shortened && o.rate_test && s.iterations >= o.min_iterations) {
+                const double th = jmax(s.rate, rate_k);
+                if (s.stepnorm > 0.0 && th < 1.0)
+                    contracted = __dmul_rn(__ddiv_rn(th, __dsub_rn(1.0, th)), s.stepnorm) <=
+                                 __dmul_rn(o.kappa, jmax(o.x_abstol, __dmul_rn(o.x_reltol, xnorm)));
+            }
+            bool stepc = false;
+            if (steptested && s.iterations >= o.min_iterations) {
+                stepc = s.iterations > 0 && s.stepnorm > 0.0 &&
+                        s.stepnorm <= jmax(o.x_abstol, __dmul_rn(o.x_reltol, xnorm));
+                stepc = stepc || (info.code == SUCCESS && info.stepnorm == 0.0);
+                stepc = stepc || (o.roundoff && s.rate >= 1.0 && rate_k < 1.0);
+            }
+            if (contracted || stepc) {
+                s.code = contracted ? SUCCESS : STALLED;
+                s.stationary = false;
+                s.contracted = contracted;
+                return s;
+            }
+            if (info.code == STALLED) {
+                stalls += 1;
+                if (stalls >= o.max_stalls) {
+                    s.code = STALLED;
+                    s.stationary = false;
+                    s.contracted = false;
+                    return s;
+                }
+            } else {
+                stalls = 0;
+            }
+            if (s.iterations >= o.max_iterations) {
+                s.code = MAXITERS;
+                s.stationary = false;
+                s.contracted = false;
+                return s;
+            }
+        }
+    }
+};
+
+}  // namespace gsb

@@ -1,0 +1,8 @@
+// Warp-form kernels of the cubic-affine family at n = 16 (16 lanes per system).
+#include "gsb_kernel_impl.cuh"
+
+namespace gsb {
+KernelEntry* warp_cubic16(bool fused, bool mixed, bool refine) {
+    return pick_warp<WarpCubic<16>, 16>(fused, mixed, refine);
+}
+}  // namespace gsb

@@ -35,6 +35,7 @@ from .api import (
     status_buffer,
     statuses,
 )
-from .batch import batch_summary, solve_batch
+from .batch import batch_summary, ragged_offsets, solve_batch, solve_batch_uneven
+from . import tune
 
 __all__ = [name for name in dir() if not name.startswith("_")]

@@ -135,6 +135,14 @@ class GsbTally(ctypes.Structure):
     _fields_ = [("counts", ctypes.c_int64 * 6)]
 
 
+class GsbBucketConfig(ctypes.Structure):
+    _fields_ = [("threads_per_system", ctypes.c_int32), ("ctas_per_sm", ctypes.c_int32)]
+
+
+GSB_UNEVEN_BUCKETS = 9
+UNEVEN_SIZES = (2, 3, 4, 6, 8, 12, 16, 24, 32)
+
+
 class GsbSummary(ctypes.Structure):
     _fields_ = [
         ("fnorm", ctypes.c_double),
@@ -164,6 +172,8 @@ EXPORTED_SYMBOLS = (
     "gsb_batch_summary",
     "gsb_synchronize",
     "gsb_solve_batch_counts_noalloc",
+    "gsb_uneven_sizes",
+    "gsb_solve_batch_uneven",
 )
 
 _lib = None
@@ -207,5 +217,13 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         ctypes.c_int64, ctypes.c_void_p, P(GsbTally),
     ]
     lib.gsb_solve_batch_counts_noalloc.restype = ctypes.c_int
+    lib.gsb_uneven_sizes.argtypes = [ctypes.POINTER(ctypes.c_int32)]
+    lib.gsb_uneven_sizes.restype = ctypes.c_int
+    lib.gsb_solve_batch_uneven.argtypes = [
+        P(GsbMethod), P(GsbOptions), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
+        ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
+        ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+    ]
+    lib.gsb_solve_batch_uneven.restype = ctypes.c_int
     _lib = lib
     return lib

@@ -2,6 +2,7 @@
 
 solve_batch(X, S, prob, method, p=None; order, options, **kwargs) -> S      batched.jl:257-287
 solve_batch(X, prob, method, p=None; ...) -> ReturnCodeCounts               batched.jl:289-307
+solve_batch_uneven(X, S, sizes, P, method; ...) -> S   systems of different sizes in one call
 Like the reference's `_launch!` (src/nonlinear/batched.jl:183-195) every call waits for its
 kernel before it returns. Host checks raise before any launch, with the reference's messages.
 """
@@ -170,3 +171,86 @@ def batch_summary(S, stream=None) -> BatchSummary:
                                          ctypes.byref(out)), lib)
     return BatchSummary(out.fnorm, bool(out.all_converged), int(out.failure_count),
                         int(out.max_iterations), int(out.total_iterations))
+
+
+def ragged_offsets(sizes):
+    """The offsets (in doubles) of each system's iterate and cubic-affine parameter block in the
+    packed X and P of a ragged batch: exclusive prefix sums of n and n^2 + n."""
+    import torch
+
+    n = sizes.to(torch.int64)
+    x_off = torch.cumsum(n, 0) - n
+    pl = n * n + n
+    p_off = torch.cumsum(pl, 0) - pl
+    return x_off.contiguous(), p_off.contiguous()
+
+
+def solve_batch_uneven(X, S, sizes, P, method, *, x_off=None, p_off=None, table=None,
+                       options=None, stream=None, **kwargs):
+    """Solve a ragged batch of cubic-affine systems in place: system s has sizes[s] unknowns
+    (from {2, 3, 4, 6, 8, 12, 16, 24, 32}); its iterate is X[x_off[s] : x_off[s] + n] of the
+    packed float64 vector X and its parameter block (A column-major, then b) is P[p_off[s] :
+    p_off[s] + n^2 + n]. S is a (nsys, 72) uint8 status tensor, or None for the count form (the
+    six return-code counts are returned). `table` is a list of nine (threads_per_system,
+    ctas_per_sm) pairs, one per size (see ``tune.autotune_uneven``); None takes the defaults.
+    The offsets default to the back-to-back packing of ``ragged_offsets``."""
+    import torch
+
+    _check_device_f64(X, "X")
+    _check_device_f64(P, "P")
+    if X.dim() != 1 or P.dim() != 1:
+        raise DimensionMismatch("X and P of a ragged batch are packed 1-D vectors")
+    if not (isinstance(sizes, torch.Tensor) and sizes.dim() == 1):
+        raise ArgumentError("sizes must be a 1-D integer tensor")
+    nsys = sizes.numel()
+    n_dev = sizes.to(device=X.device, dtype=torch.int32).contiguous()
+    if x_off is None or p_off is None:
+        xo, po = ragged_offsets(n_dev)
+        x_off = xo if x_off is None else x_off
+        p_off = po if p_off is None else p_off
+    x_off = torch.as_tensor(x_off).to(device=X.device, dtype=torch.int64).contiguous()
+    p_off = torch.as_tensor(p_off).to(device=X.device, dtype=torch.int64).contiguous()
+    if x_off.numel() != nsys or p_off.numel() != nsys:
+        raise DimensionMismatch("x_off and p_off must have one entry per system")
+    if nsys:
+        n64 = n_dev.to(torch.int64)
+        if int((x_off + n64).max()) > X.numel() or int(x_off.min()) < 0:
+            raise DimensionMismatch("an iterate reaches outside X")
+        if int((p_off + n64 * n64 + n64).max()) > P.numel() or int(p_off.min()) < 0:
+            raise DimensionMismatch("a parameter block reaches outside P")
+    opt = _resolve_options(options, kwargs)
+    counts_form = S is None
+    if counts_form:
+        S_buf = torch.empty(nsys, dtype=torch.uint8, device=X.device)
+        s_kind = abi.GSB_CODES
+    else:
+        if not (isinstance(S, torch.Tensor) and S.dtype == torch.uint8 and S.is_cuda):
+            raise ArgumentError("S must be a (nsys, 72) uint8 CUDA tensor (status_buffer)")
+        if S.numel() != nsys * 72:
+            raise DimensionMismatch(
+                f"status vector length {S.numel() // 72} does not match batch length {nsys}")
+        S_buf = S
+        s_kind = abi.GSB_STATUS64
+    tab = None
+    if table is not None:
+        if len(table) != abi.GSB_UNEVEN_BUCKETS:
+            raise ArgumentError(f"table takes {abi.GSB_UNEVEN_BUCKETS} entries")
+        tab = (abi.GsbBucketConfig * abi.GSB_UNEVEN_BUCKETS)(
+            *[abi.GsbBucketConfig(int(t), int(c)) for t, c in table])
+    gm, go = method.to_abi(), opt.to_abi()
+    if nsys == 0:
+        return ReturnCodeCounts(0, 0, 0, 0, 0, 0) if counts_form else S
+    lib = abi.load_library()
+    if stream is None:
+        stream = torch.cuda.current_stream(X.device)
+    tally = abi.GsbTally()
+    with torch.cuda.device(X.device):
+        rc = lib.gsb_solve_batch_uneven(
+            ctypes.byref(gm), ctypes.byref(go), X.data_ptr(), S_buf.data_ptr(), s_kind,
+            P.data_ptr(), n_dev.data_ptr(), x_off.data_ptr(), p_off.data_ptr(), nsys,
+            None if tab is None else ctypes.cast(tab, ctypes.c_void_p),
+            ctypes.c_void_p(stream.cuda_stream), ctypes.byref(tally))
+        _raise_for(rc, lib)
+    if counts_form:
+        return ReturnCodeCounts(*[int(c) for c in tally.counts])
+    return S

@@ -29,7 +29,58 @@ struct Launch {
     int64_t nsys;
     const double* shared;
     unsigned long long* tally;  // 6 counters or nullptr
+    // Ragged batches (systems of different sizes packed back to back): the offsets, in doubles,
+    // of each system's iterate in X and parameter block in P, indexed like S; nullptr for the
+    // uniform layouts.
+    const int64_t* x_off;
+    const int64_t* p_off;
+    // Persistent launches: a counter of CTA-sized chunks taken so far (zero at launch); nullptr
+    // for one chunk per CTA.
+    unsigned long long* queue;
+    // A bucket of a ragged batch: {count, first} in device memory, written on the device before
+    // the launch; the launch then solves order[first .. first + count) instead of order[0 ..
+    // nsys). nullptr otherwise.
+    const unsigned long long* bucket;
 };
+
+// The systems a launch solves: `n` entries of `order` (or 0 .. n-1 without one).
+struct Range {
+    int64_t n;
+    const int64_t* order;
+};
+
+__device__ __forceinline__ Range launch_range(const Launch& L) {
+    if (L.bucket) return {(int64_t)L.bucket[0], L.order + L.bucket[1]};
+    return {L.nsys, L.order};
+}
+
+// The CTA's chunks: one per CTA, or, with a work queue, chunks taken from the counter until the
+// batch is exhausted (systems_per_chunk systems each).
+template <class Body>
+__device__ __forceinline__ void for_each_chunk(const Launch& L, int64_t systems_per_chunk, Body body) {
+    const Range r = launch_range(L);
+    if (L.queue == nullptr) {
+        body((int64_t)blockIdx.x * systems_per_chunk, r);
+        return;
+    }
+    __shared__ unsigned long long next;
+    while (true) {
+        if (threadIdx.x == 0) next = atomicAdd(L.queue, 1ull);
+        __syncthreads();
+        const int64_t base = (int64_t)next * systems_per_chunk;
+        __syncthreads();  // every thread holds `next` before thread 0 takes the following chunk
+        if (base >= r.n) return;
+        body(base, r);
+        __syncthreads();  // the chunk's shared memory is free again
+    }
+}
+
+__device__ __forceinline__ const double* param_block(const Launch& L, int64_t idx, int np) {
+    return L.p_off ? L.P + L.p_off[idx] : L.P + idx * np;
+}
+__device__ __forceinline__ double* x_block(const Launch& L, int64_t idx, int n) {
+    return L.x_off ? L.X + L.x_off[idx] : L.X + idx * n;
+}
 
 // Row of a thread's shared memory: its parameter block (np doubles), then 2n doubles where the
 // iterate and the residual wait while a factor holds the registers; the stride is odd, so that
@@ -74,8 +125,13 @@ __device__ __forceinline__ void tally_code(unsigned long long* tally, int code) 
 // rows of stride RS in shared memory. Each thread issues all of its loads before any store, in
 // batches of 16, so that the HBM round trips of one thread overlap instead of following one
 // another.
-template <int NP, int RS, int ROWS>
-__device__ __forceinline__ void stage_aos(double* smem, const double* src, int64_t rows_left, int tid) {
+struct IdentityPlace {
+    __device__ __forceinline__ int operator()(int k) const { return k; }
+};
+
+template <int NP, int RS, int ROWS, class Place = IdentityPlace>
+__device__ __forceinline__ void stage_aos(double* smem, const double* src, int64_t rows_left, int tid,
+                                          Place place = Place()) {
     constexpr int TOTAL = ROWS * NP;
     constexpr int PER = (TOTAL + kThreads - 1) / kThreads;
     constexpr int BATCH = 16;
@@ -93,7 +149,7 @@ __device__ __forceinline__ void stage_aos(double* smem, const double* src, int64
             const int q = (b0 + b) * kThreads + tid;
             if (b0 + b < PER && q < total) {
                 const int s = q / NP;
-                smem[s * RS + (q - s * NP)] = v[b];
+                smem[s * RS + place(q - s * NP)] = v[b];
             }
         }
     }
@@ -116,40 +172,43 @@ __global__ void __launch_bounds__(kThreads, (min_blocks<Fam, Mixed>())) newton_k
     extern __shared__ double smem[];
     constexpr int N = Fam::N, NP = Fam::NP, RS = row_stride(NP, N);
     const int tid = threadIdx.x;
-    const int64_t base = (int64_t)blockIdx.x * blockDim.x;
-    const int64_t i = base + tid;
     double* prow = smem + tid * RS;
-    if (L.order == nullptr && L.p_layout == GSB_AOS) {
-        stage_aos<NP, RS, kThreads>(smem, L.P + base * NP, L.nsys - base, tid);
-    } else if (i < L.nsys) {
-        int64_t idx = L.order ? L.order[i] - L.order_base : i;
-        if (L.p_layout == GSB_SOA) {
+    for_each_chunk(L, kThreads, [&](int64_t base, const Range& r) {
+        const int64_t i = base + tid;
+        if (r.order == nullptr && L.p_layout == GSB_AOS && L.p_off == nullptr) {
+            stage_aos<NP, RS, kThreads>(smem, L.P + base * NP, r.n - base, tid);
+        } else if (i < r.n) {
+            const int64_t idx = r.order ? r.order[i] - L.order_base : i;
+            if (L.p_layout == GSB_SOA) {
 #pragma unroll 4
-            for (int k = 0; k < NP; ++k) prow[k] = __ldg(L.P + (int64_t)k * L.nsys + idx);
-        } else {
+                for (int k = 0; k < NP; ++k) prow[k] = __ldg(L.P + (int64_t)k * L.nsys + idx);
+            } else {
+                const double* pb = param_block(L, idx, NP);
 #pragma unroll 4
-            for (int k = 0; k < NP; ++k) prow[k] = __ldg(L.P + idx * NP + k);
+                for (int k = 0; k < NP; ++k) prow[k] = __ldg(pb + k);
+            }
         }
-    }
-    __syncthreads();
-    if (i >= L.nsys) return;
-    const int64_t idx = L.order ? L.order[i] - L.order_base : i;
-    Fam fam{prow};
-    double x[N];
+        __syncthreads();
+        if (i >= r.n) return;
+        const int64_t idx = r.order ? r.order[i] - L.order_base : i;
+        Fam fam{prow};
+        double x[N];
+        double* xb = x_block(L, idx, N);
 #pragma unroll
-    for (int k = 0; k < N; ++k)
-        x[k] = L.x_layout == GSB_SOA ? L.X[(int64_t)k * L.nsys + idx] : L.X[idx * N + k];
-    Solver<Fam, F, Mixed, PlainRef> sv(fam, m, o, N >= 6 ? prow + NP : nullptr);
-    double gr;
-    DevStatus s = sv.solve(x, gr);
+        for (int k = 0; k < N; ++k)
+            x[k] = L.x_layout == GSB_SOA ? L.X[(int64_t)k * L.nsys + idx] : xb[k];
+        Solver<Fam, F, Mixed, PlainRef> sv(fam, m, o, N >= 6 ? prow + NP : nullptr);
+        double gr;
+        DevStatus s = sv.solve(x, gr);
 #pragma unroll
-    for (int k = 0; k < N; ++k) {
-        if (L.x_layout == GSB_SOA) L.X[(int64_t)k * L.nsys + idx] = x[k];
-        else L.X[idx * N + k] = x[k];
-    }
-    if (L.s_kind == GSB_STATUS64) store_status(L.S, idx, s, gr);
-    else reinterpret_cast<unsigned char*>(L.S)[idx] = (unsigned char)s.code;
-    if (L.tally) tally_code(L.tally, s.code);
+        for (int k = 0; k < N; ++k) {
+            if (L.x_layout == GSB_SOA) L.X[(int64_t)k * L.nsys + idx] = x[k];
+            else xb[k] = x[k];
+        }
+        if (L.s_kind == GSB_STATUS64) store_status(L.S, idx, s, gr);
+        else reinterpret_cast<unsigned char*>(L.S)[idx] = (unsigned char)s.code;
+        if (L.tally) tally_code(L.tally, s.code);
+    });
 }
 
 
@@ -162,41 +221,42 @@ __global__ void __launch_bounds__(kThreads) team_kernel(GsbMethod m, GsbOptions 
     constexpr int SPB = kThreads / T;
     const int tid = threadIdx.x;
     const int team = tid / T;
-    const int64_t base = (int64_t)blockIdx.x * SPB;
-    const int64_t i = base + team;
-    if (L.order == nullptr && L.p_layout == GSB_AOS) {
-        stage_aos<NP, RS, SPB>(smem, L.P + base * NP, L.nsys - base, tid);
-    } else if (i < L.nsys) {
-        const int64_t idx = L.order ? L.order[i] - L.order_base : i;
-        double* prow = smem + team * RS;
-        for (int k = tid % T; k < NP; k += T)
-            prow[k] = L.p_layout == GSB_SOA ? __ldg(L.P + (int64_t)k * L.nsys + idx)
-                                            : __ldg(L.P + idx * NP + k);
-    }
-    __syncthreads();
-    if (i >= L.nsys) return;
-    const int64_t idx = L.order ? L.order[i] - L.order_base : i;
-    Fam fam{smem + team * RS};
-    double x[N];
+    for_each_chunk(L, SPB, [&](int64_t base, const Range& r) {
+        const int64_t i = base + team;
+        if (r.order == nullptr && L.p_layout == GSB_AOS && L.p_off == nullptr) {
+            stage_aos<NP, RS, SPB>(smem, L.P + base * NP, r.n - base, tid);
+        } else if (i < r.n) {
+            const int64_t idx = r.order ? r.order[i] - L.order_base : i;
+            double* prow = smem + team * RS;
+            const double* pb = param_block(L, idx, NP);
+            for (int k = tid % T; k < NP; k += T)
+                prow[k] = L.p_layout == GSB_SOA ? __ldg(L.P + (int64_t)k * L.nsys + idx) : __ldg(pb + k);
+        }
+        __syncthreads();
+        if (i >= r.n) return;
+        const int64_t idx = r.order ? r.order[i] - L.order_base : i;
+        Fam fam{smem + team * RS};
+        double* xb = x_block(L, idx, N);
+        double x[N];
 #pragma unroll
-    for (int k = 0; k < N; ++k)
-        x[k] = L.x_layout == GSB_SOA ? L.X[(int64_t)k * L.nsys + idx] : L.X[idx * N + k];
-    TeamSolver<Fam, T, Mixed> sv(fam, m, o);
-    double gr;
-    DevStatus s = sv.solve(x, gr);
-    const int lane = tid % T;
+        for (int k = 0; k < N; ++k) x[k] = L.x_layout == GSB_SOA ? L.X[(int64_t)k * L.nsys + idx] : xb[k];
+        TeamSolver<Fam, T, Mixed> sv(fam, m, o);
+        double gr;
+        DevStatus s = sv.solve(x, gr);
+        const int lane = tid % T;
 #pragma unroll
-    for (int q = 0; q < N / T; ++q) {
-        const int k = q * T + lane;
-        const double v = own<N, T>(x, q, lane);
-        if (L.x_layout == GSB_SOA) L.X[(int64_t)k * L.nsys + idx] = v;
-        else L.X[idx * N + k] = v;
-    }
-    if (lane == 0) {
-        if (L.s_kind == GSB_STATUS64) store_status(L.S, idx, s, gr);
-        else reinterpret_cast<unsigned char*>(L.S)[idx] = (unsigned char)s.code;
-        if (L.tally) tally_code(L.tally, s.code);
-    }
+        for (int q = 0; q < N / T; ++q) {
+            const int k = q * T + lane;
+            const double v = own<N, T>(x, q, lane);
+            if (L.x_layout == GSB_SOA) L.X[(int64_t)k * L.nsys + idx] = v;
+            else xb[k] = v;
+        }
+        if (lane == 0) {
+            if (L.s_kind == GSB_STATUS64) store_status(L.S, idx, s, gr);
+            else reinterpret_cast<unsigned char*>(L.S)[idx] = (unsigned char)s.code;
+            if (L.tally) tally_code(L.tally, s.code);
+        }
+    });
 }
 
 // The least-squares form: one Levenberg–Marquardt solve per thread. Shared memory holds each
@@ -245,10 +305,16 @@ __global__ void __launch_bounds__(kThreads, 3) lm_kernel(GsbMethod m, GsbOptions
 }
 
 // The warp form (n = 12 ... 32): T lanes per system, kThreads / T systems per CTA. Each system's
-// shared memory holds its parameter block, then its N x LD factor.
+// shared memory holds its parameter block in the family's layout (SP doubles), then its N x LD
+// factor.
 template <class Fam> __host__ __device__ constexpr int warp_sys_stride() {
-    return ((Fam::NP + 1) / 2) * 2 + Fam::N * warp_ld(Fam::N);
+    return ((Fam::SP + 1) / 2) * 2 + Fam::N * warp_ld(Fam::N);
 }
+
+// Parameter k of a system to its place in the family's shared-memory layout.
+template <class Fam> struct WarpPlace {
+    __device__ __forceinline__ int operator()(int k) const { return Fam::place(k); }
+};
 
 template <class Fam, int T, bool F, bool Mixed, bool PlainRef>
 __global__ void __launch_bounds__(kThreads) warp_kernel(GsbMethod m, GsbOptions o, Launch L) {
@@ -256,37 +322,40 @@ __global__ void __launch_bounds__(kThreads) warp_kernel(GsbMethod m, GsbOptions 
     constexpr int N = Fam::N, NP = Fam::NP, SPB = kThreads / T, SS = warp_sys_stride<Fam>();
     const int tid = threadIdx.x;
     const int team = tid / T;
-    const int64_t base = (int64_t)blockIdx.x * SPB;
-    const int64_t i = base + team;
     double* sys = smem + team * SS;
-    if (L.order == nullptr && L.p_layout == GSB_AOS) {
-        stage_aos<NP, SS, SPB>(smem, L.P + base * NP, L.nsys - base, tid);
-    } else if (i < L.nsys) {
-        const int64_t idx = L.order ? L.order[i] - L.order_base : i;
-        for (int k = tid % T; k < NP; k += T)
-            sys[k] = L.p_layout == GSB_SOA ? __ldg(L.P + (int64_t)k * L.nsys + idx)
-                                           : __ldg(L.P + idx * NP + k);
-    }
-    __syncthreads();
-    if (i >= L.nsys) return;
-    const int64_t idx = L.order ? L.order[i] - L.order_base : i;
-    Team<T> tm;
-    const int lane = tm.lane;
-    Fam fam{sys};
-    double xl = 0.0;
-    if (lane < N) xl = L.x_layout == GSB_SOA ? L.X[(int64_t)lane * L.nsys + idx] : L.X[idx * N + lane];
-    WarpSolver<Fam, T, F, Mixed, PlainRef> sv(fam, m, o, tm, sys + ((NP + 1) / 2) * 2);
-    double gr;
-    DevStatus s = sv.solve(xl, gr);
-    if (lane < N) {
-        if (L.x_layout == GSB_SOA) L.X[(int64_t)lane * L.nsys + idx] = xl;
-        else L.X[idx * N + lane] = xl;
-    }
-    if (lane == 0) {
-        if (L.s_kind == GSB_STATUS64) store_status(L.S, idx, s, gr);
-        else reinterpret_cast<unsigned char*>(L.S)[idx] = (unsigned char)s.code;
-        if (L.tally) tally_code(L.tally, s.code);
-    }
+    for_each_chunk(L, SPB, [&](int64_t base, const Range& r) {
+        const int64_t i = base + team;
+        if (r.order == nullptr && L.p_layout == GSB_AOS && L.p_off == nullptr) {
+            stage_aos<NP, SS, SPB>(smem, L.P + base * NP, r.n - base, tid, WarpPlace<Fam>());
+        } else if (i < r.n) {
+            const int64_t idx = r.order ? r.order[i] - L.order_base : i;
+            const double* pb = param_block(L, idx, NP);
+            for (int k = tid % T; k < NP; k += T)
+                sys[Fam::place(k)] = L.p_layout == GSB_SOA ? __ldg(L.P + (int64_t)k * L.nsys + idx)
+                                                           : __ldg(pb + k);
+        }
+        __syncthreads();
+        if (i >= r.n) return;
+        const int64_t idx = r.order ? r.order[i] - L.order_base : i;
+        Team<T> tm;
+        const int lane = tm.lane;
+        Fam fam{sys};
+        double* xb = x_block(L, idx, N);
+        double xl = 0.0;
+        if (lane < N) xl = L.x_layout == GSB_SOA ? L.X[(int64_t)lane * L.nsys + idx] : xb[lane];
+        WarpSolver<Fam, T, F, Mixed, PlainRef> sv(fam, m, o, tm, sys + ((Fam::SP + 1) / 2) * 2);
+        double gr;
+        DevStatus s = sv.solve(xl, gr);
+        if (lane < N) {
+            if (L.x_layout == GSB_SOA) L.X[(int64_t)lane * L.nsys + idx] = xl;
+            else xb[lane] = xl;
+        }
+        if (lane == 0) {
+            if (L.s_kind == GSB_STATUS64) store_status(L.S, idx, s, gr);
+            else reinterpret_cast<unsigned char*>(L.S)[idx] = (unsigned char)s.code;
+            if (L.tally) tally_code(L.tally, s.code);
+        }
+    });
 }
 
 using KernelFn = void (*)(GsbMethod, GsbOptions, Launch);

@@ -8,6 +8,7 @@
 // writes its iterate and its 72-byte status.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -174,10 +175,10 @@ GSB_DECLARE_ENTRY(coupled2);
 GSB_DECLARE_TEAM(cubic6);
 GSB_DECLARE_TEAM(cubic8);
 KernelEntry* lm_expsum3_64(bool fused);
-KernelEntry* warp_cubic12(bool fused, bool mixed, bool refine);
-KernelEntry* warp_cubic16(bool fused, bool mixed, bool refine);
-KernelEntry* warp_cubic24(bool fused, bool mixed, bool refine);
-KernelEntry* warp_cubic32(bool fused, bool mixed, bool refine);
+KernelEntry* warp_cubic12(bool fused, bool mixed, bool refine, int T);
+KernelEntry* warp_cubic16(bool fused, bool mixed, bool refine, int T);
+KernelEntry* warp_cubic24(bool fused, bool mixed, bool refine, int T);
+KernelEntry* warp_cubic32(bool fused, bool mixed, bool refine, int T);
 }  // namespace gsb
 
 namespace {
@@ -195,14 +196,14 @@ int tuned_team(const GsbProblem* prob, bool mixed) {
 // The kernel of a call: the one-thread solve for T = 1, else the team solve (fused only).
 KernelEntry* select_kernel(const GsbProblem* prob, bool fused, bool mixed, bool refine, int T) {
     if (prob->family == GSB_FAMILY_CUBIC_AFFINE && prob->n >= 12) {
-        // the warp form: 16 lanes per system up to n = 16, a whole warp above
-        const int tw = prob->n <= 16 ? 16 : 32;
-        if (T != 0 && T != tw) return nullptr;
+        // the warp form: 16 lanes per system up to n = 16 (or a whole warp), a whole warp above
+        if (T == 0) T = prob->n <= 16 ? 16 : 32;
+        if (!(T == 32 || (T == 16 && prob->n <= 16))) return nullptr;
         switch (prob->n) {
-        case 12: return warp_cubic12(fused, mixed, refine);
-        case 16: return warp_cubic16(fused, mixed, refine);
-        case 24: return warp_cubic24(fused, mixed, refine);
-        case 32: return warp_cubic32(fused, mixed, refine);
+        case 12: return warp_cubic12(fused, mixed, refine, T);
+        case 16: return warp_cubic16(fused, mixed, refine, T);
+        case 24: return warp_cubic24(fused, mixed, refine, T);
+        case 32: return warp_cubic32(fused, mixed, refine, T);
         default: return nullptr;
         }
     }
@@ -613,6 +614,290 @@ int gsb_solve_batch_counts_noalloc(const GsbProblem* prob, const GsbMethod* meth
         return rc;
     if (int rc = cuda_err(cudaStreamSynchronize(st), "tally copy")) return rc;
     for (int c = 0; c < 6; ++c) tally->counts[c] = (int64_t)h[c];
+    return 0;
+}
+
+}  // extern "C"
+
+// ─── ragged batches ─────────────────────────────────────────────────────────────────────────
+//
+// Systems of different sizes, packed back to back. Three small kernels sort the systems into
+// size buckets (count, ranges, scatter of the indices), then each bucket's kernel, a persistent
+// launch with its own device work queue, solves its bucket through `order` and the ragged
+// offsets. The buckets' kernels run on forked streams, so their tails overlap; the whole
+// sequence is captured once into a CUDA graph per set of arguments and replayed.
+
+namespace gsb {
+
+constexpr int kUnevenSizes[GSB_UNEVEN_BUCKETS] = {2, 3, 4, 6, 8, 12, 16, 24, 32};
+
+__device__ __forceinline__ int uneven_bucket(int n) {
+    switch (n) {
+    case 2: return 0;
+    case 3: return 1;
+    case 4: return 2;
+    case 6: return 3;
+    case 8: return 4;
+    case 12: return 5;
+    case 16: return 6;
+    case 24: return 7;
+    case 32: return 8;
+    default: return -1;
+    }
+}
+
+// The bucketing state of one call, in device memory (zeroed at the start of each run).
+struct UnevenWork {
+    unsigned long long count[GSB_UNEVEN_BUCKETS];
+    unsigned long long cursor[GSB_UNEVEN_BUCKETS];
+    unsigned long long range[GSB_UNEVEN_BUCKETS][2];  // {count, first} in the index list
+    unsigned long long queue[GSB_UNEVEN_BUCKETS];
+    unsigned long long bad;  // systems whose size is outside the set
+    unsigned long long tally[6];
+};
+
+// Sizes to bucket counts, one atomic per bucket present in a warp.
+__global__ void uneven_count(const int32_t* n, int64_t nsys, UnevenWork* w) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < nsys; s += stride) {
+        const int b = uneven_bucket(n[s]);
+        const unsigned act = __activemask();
+        const unsigned grp = __match_any_sync(act, b);
+        if ((threadIdx.x & 31) == __ffs(grp) - 1) {
+            if (b < 0) atomicAdd(&w->bad, (unsigned long long)__popc(grp));
+            else atomicAdd(&w->count[b], (unsigned long long)__popc(grp));
+        }
+    }
+}
+
+// Bucket b's indices start after those of the smaller sizes.
+__global__ void uneven_ranges(UnevenWork* w) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    unsigned long long first = 0;
+    for (int b = 0; b < GSB_UNEVEN_BUCKETS; ++b) {
+        w->range[b][0] = w->count[b];
+        w->range[b][1] = first;
+        first += w->count[b];
+    }
+}
+
+// Each system's index into its bucket's part of the list (the order within a bucket is that of
+// the atomics; every system is solved alone, so it does not change any result).
+__global__ void uneven_scatter(const int32_t* n, int64_t nsys, UnevenWork* w, int64_t* list) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    const int lane = threadIdx.x & 31;
+    for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < nsys; s += stride) {
+        const int b = uneven_bucket(n[s]);
+        const unsigned act = __activemask();
+        const unsigned grp = __match_any_sync(act, b);
+        const int leader = __ffs(grp) - 1;
+        unsigned long long at = 0;
+        if (lane == leader && b >= 0) at = atomicAdd(&w->cursor[b], (unsigned long long)__popc(grp));
+        at = __shfl_sync(grp, at, leader);
+        if (b >= 0) {
+            const unsigned below = grp & ((1u << lane) - 1u);
+            list[w->range[b][1] + at + __popc(below)] = s;
+        }
+    }
+}
+
+}  // namespace gsb
+
+namespace {
+
+struct UnevenKey {
+    GsbMethod m;
+    GsbOptions o;
+    GsbBucketConfig table[GSB_UNEVEN_BUCKETS];
+    double* X;
+    void* S;
+    int32_t s_kind;
+    const double* P;
+    const int32_t* n;
+    const int64_t* x_off;
+    const int64_t* p_off;
+    int64_t nsys;
+    bool operator==(const UnevenKey& k) const { return std::memcmp(this, &k, sizeof(*this)) == 0; }
+};
+
+// One device's ragged-batch state: the bucketing workspace, the streams of the buckets' fork,
+// and the graph of the last argument set.
+struct UnevenPlan {
+    bool ready = false;
+    UnevenKey key{};
+    gsb::UnevenWork* work = nullptr;
+    int64_t* list = nullptr;
+    int64_t list_cap = 0;
+    cudaStream_t cs = nullptr;
+    cudaStream_t side[GSB_UNEVEN_BUCKETS] = {};
+    cudaEvent_t fork = nullptr;
+    cudaEvent_t join[GSB_UNEVEN_BUCKETS] = {};
+    cudaGraphExec_t exec = nullptr;
+};
+std::mutex g_uneven_mu;
+UnevenPlan g_uneven[64];
+
+int uneven_streams(UnevenPlan& p) {
+    if (p.cs) return 0;
+    if (int rc = cuda_err(cudaStreamCreateWithFlags(&p.cs, cudaStreamNonBlocking), "stream")) return rc;
+    if (int rc = cuda_err(cudaEventCreateWithFlags(&p.fork, cudaEventDisableTiming), "event")) return rc;
+    for (int b = 0; b < GSB_UNEVEN_BUCKETS; ++b) {
+        if (int rc = cuda_err(cudaStreamCreateWithFlags(&p.side[b], cudaStreamNonBlocking), "stream"))
+            return rc;
+        if (int rc = cuda_err(cudaEventCreateWithFlags(&p.join[b], cudaEventDisableTiming), "event"))
+            return rc;
+    }
+    return 0;
+}
+
+// The kernel of bucket b and its persistent grid; nullptr when the combination has no kernel.
+int uneven_entry(const UnevenKey& k, int b, int sms, KernelEntry** ke, unsigned* grid) {
+    GsbProblem prob{};
+    prob.family = GSB_FAMILY_CUBIC_AFFINE;
+    prob.n = prob.m = kUnevenSizes[b];
+    const bool fused = k.m.arithmetic == GSB_FUSED;
+    const bool mixed = k.m.factor_precision == GSB_F32;
+    const int T = k.table[b].threads_per_system;
+    *ke = select_kernel(&prob, fused, mixed, k.m.refinement == GSB_REFINEMENT,
+                        T == 0 ? (kUnevenSizes[b] <= 8 ? 1 : 0) : T);
+    if (!*ke) return set_err(GSB_ERR_UNSUPPORTED, "no kernel for bucket n = " +
+                                                      std::to_string(kUnevenSizes[b]) +
+                                                      " with these threads per system");
+    const size_t smem = (size_t)(*ke)->smem_doubles * sizeof(double);
+    int dev = 0;
+    if (int rc = cuda_err(cudaGetDevice(&dev), "cudaGetDevice")) return rc;
+    if (!(*ke)->attr_set[dev & 63]) {
+        if (int rc = cuda_err(cudaFuncSetAttribute(reinterpret_cast<const void*>((*ke)->fn),
+                                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   (int)smem), "cudaFuncSetAttribute"))
+            return rc;
+        (*ke)->attr_set[dev & 63] = true;
+    }
+    int occ = 0;
+    if (int rc = cuda_err(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                              &occ, reinterpret_cast<const void*>((*ke)->fn), kThreads, smem),
+                          "occupancy"))
+        return rc;
+    if (occ < 1) return set_err(GSB_ERR_UNSUPPORTED, "a bucket kernel does not fit on an SM");
+    const int want = k.table[b].ctas_per_sm;
+    *grid = (unsigned)((want > 0 && want < occ ? want : occ) * sms);
+    return 0;
+}
+
+int uneven_capture(UnevenPlan& p, const UnevenKey& k, bool want_tally) {
+    int dev = 0, sms = 0;
+    if (int rc = cuda_err(cudaGetDevice(&dev), "cudaGetDevice")) return rc;
+    if (int rc = cuda_err(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "attr"))
+        return rc;
+    KernelEntry* ke[GSB_UNEVEN_BUCKETS];
+    unsigned grid[GSB_UNEVEN_BUCKETS];
+    for (int b = 0; b < GSB_UNEVEN_BUCKETS; ++b)
+        if (int rc = uneven_entry(k, b, sms, &ke[b], &grid[b])) return rc;
+    if (p.exec) {
+        cudaGraphExecDestroy(p.exec);
+        p.exec = nullptr;
+    }
+    const unsigned cgrid = (unsigned)std::min<int64_t>((k.nsys + 255) / 256, (int64_t)sms * 8);
+    cudaGraph_t g = nullptr;
+    if (int rc = cuda_err(cudaStreamBeginCapture(p.cs, cudaStreamCaptureModeThreadLocal), "capture"))
+        return rc;
+    cudaMemsetAsync(p.work, 0, sizeof(gsb::UnevenWork), p.cs);
+    gsb::uneven_count<<<cgrid, 256, 0, p.cs>>>(k.n, k.nsys, p.work);
+    gsb::uneven_ranges<<<1, 32, 0, p.cs>>>(p.work);
+    gsb::uneven_scatter<<<cgrid, 256, 0, p.cs>>>(k.n, k.nsys, p.work, p.list);
+    cudaEventRecord(p.fork, p.cs);
+    // the heaviest buckets (largest n) start first, so that the light ones fill the tail
+    for (int b = GSB_UNEVEN_BUCKETS - 1; b >= 0; --b) {
+        cudaStreamWaitEvent(p.side[b], p.fork, 0);
+        Launch L{k.X, GSB_AOS, k.S, k.s_kind, k.P, GSB_AOS, p.list, 0, k.nsys, nullptr,
+                 want_tally ? p.work->tally : nullptr, k.x_off, k.p_off, &p.work->queue[b],
+                 &p.work->range[b][0]};
+        ke[b]->fn<<<grid[b], kThreads, (size_t)ke[b]->smem_doubles * sizeof(double), p.side[b]>>>(
+            k.m, k.o, L);
+        cudaEventRecord(p.join[b], p.side[b]);
+        cudaStreamWaitEvent(p.cs, p.join[b], 0);
+    }
+    cudaError_t e = cudaStreamEndCapture(p.cs, &g);
+    if (int rc = cuda_err(e, "end capture")) return rc;
+    e = cudaGraphInstantiate(&p.exec, g, 0);
+    cudaGraphDestroy(g);
+    if (int rc = cuda_err(e, "graph instantiate")) return rc;
+    return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int gsb_uneven_sizes(int32_t* sizes_out) {
+    if (!sizes_out) return set_err(GSB_ERR_ARGUMENT, "null sizes_out");
+    for (int b = 0; b < GSB_UNEVEN_BUCKETS; ++b) sizes_out[b] = kUnevenSizes[b];
+    return 0;
+}
+
+int gsb_solve_batch_uneven(const GsbMethod* method, const GsbOptions* opt, double* X, void* S,
+                           int32_t s_kind, const double* P, const int32_t* n,
+                           const int64_t* x_off, const int64_t* p_off, int64_t nsys,
+                           const GsbBucketConfig* table, void* stream, GsbTally* tally) {
+    g_err.clear();
+    if (!method || !opt) return set_err(GSB_ERR_ARGUMENT, "null method or options");
+    if (nsys < 0) return set_err(GSB_ERR_DIMENSION, "negative batch length");
+    if (int rc = check_options(opt)) return rc;
+    if (int rc = check_method(method)) return rc;
+    if (method->globalization == GSB_LEVENBERG_MARQUARDT || method->linsolve != GSB_LU)
+        return set_err(GSB_ERR_UNSUPPORTED, "ragged batches run Newton with LUFactorization");
+    if (s_kind != GSB_STATUS64 && s_kind != GSB_CODES) return set_err(GSB_ERR_ARGUMENT, "s_kind");
+    if (tally) std::memset(tally, 0, sizeof(*tally));
+    if (nsys == 0) return 0;
+    if (!X || !S || !P || !n || !x_off || !p_off)
+        return set_err(GSB_ERR_ARGUMENT, "null X, S, P, n, x_off or p_off");
+    UnevenKey key{};
+    key.m = *method;
+    key.o = *opt;
+    if (table) std::memcpy(key.table, table, sizeof(key.table));
+    key.X = X;
+    key.S = S;
+    key.s_kind = s_kind;
+    key.P = P;
+    key.n = n;
+    key.x_off = x_off;
+    key.p_off = p_off;
+    key.nsys = nsys;
+    int dev = 0;
+    if (int rc = cuda_err(cudaGetDevice(&dev), "cudaGetDevice")) return rc;
+    if (dev < 0 || dev >= 64) return set_err(GSB_ERR_CUDA, "device index out of range");
+    std::lock_guard<std::mutex> lk(g_uneven_mu);
+    UnevenPlan& p = g_uneven[dev];
+    if (int rc = uneven_streams(p)) return rc;
+    if (!p.work) {
+        if (int rc = cuda_err(cudaMalloc(&p.work, sizeof(gsb::UnevenWork)), "cudaMalloc")) return rc;
+    }
+    if (p.list_cap < nsys) {
+        if (p.list) cudaFree(p.list);
+        p.list = nullptr;
+        p.list_cap = 0;
+        p.ready = false;
+        if (int rc = cuda_err(cudaMalloc(&p.list, nsys * sizeof(int64_t)), "cudaMalloc")) return rc;
+        p.list_cap = nsys;
+    }
+    if (!p.ready || !(p.key == key)) {
+        p.ready = false;
+        if (int rc = uneven_capture(p, key, true)) return rc;
+        p.key = key;
+        p.ready = true;
+    }
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    if (int rc = cuda_err(cudaGraphLaunch(p.exec, st), "graph launch")) return rc;
+    unsigned long long h[7];
+    if (int rc = cuda_err(cudaMemcpyAsync(h, &p.work->bad, sizeof(h), cudaMemcpyDeviceToHost, st),
+                          "tally copy"))
+        return rc;
+    if (int rc = cuda_err(cudaStreamSynchronize(st), "synchronize")) return rc;
+    if (tally)
+        for (int c = 0; c < 6; ++c) tally->counts[c] = (int64_t)h[1 + c];
+    if (h[0]) return set_err(GSB_ERR_ARGUMENT, std::to_string(h[0]) +
+                                                   " systems have a size outside {2, 3, 4, 6, 8, "
+                                                   "12, 16, 24, 32}");
     return 0;
 }
 

@@ -28,13 +28,18 @@ namespace gsb {
 __host__ __device__ constexpr int warp_ld(int n) { return (n % 2 == 1) ? n : n + 1; }
 
 // The cubic-affine family in row form: F_i(x) = (A x)_i + 0.1 x_i^3 - b_i with the one-thread
-// family's operations (gsb_families.cuh). `p` is the system's parameter block in shared memory
-// (A column-major, then b).
+// family's operations (gsb_families.cuh). `p` is the system's parameter block in shared memory:
+// A column-major with an odd column stride LDA (so that lanes reading along a row, as lanes
+// reading down a column, fall in distinct bank slots), then b.
 template <int N_> struct WarpCubic {
-    static constexpr int N = N_, NP = N_ * N_ + N_;
+    static constexpr int N = N_, NP = N_ * N_ + N_, LDA = warp_ld(N_), SP = N_ * LDA + N_;
     const double* p;
+    // place of parameter k (A column-major, then b) in the shared-memory block
+    __host__ __device__ static constexpr int place(int k) {
+        return k < N * N ? (k % N) + (k / N) * LDA : N * LDA + (k - N * N);
+    }
     __device__ __forceinline__ double par(int k) const { return lds(smem_addr(p) + 8u * k); }
-    __device__ __forceinline__ double A(int i, int k) const { return par(i + k * N); }
+    __device__ __forceinline__ double A(int i, int k) const { return par(i + k * LDA); }
 
     // Row i (< N) of F; every lane of the team calls it (x_j arrive by broadcast).
     template <int T>
@@ -44,7 +49,7 @@ template <int N_> struct WarpCubic {
 #pragma unroll 8
         for (int j = 1; j < N; ++j) t = __fma_rn(A(r, j), tm.bcast(xl, j), t);
         const double c = __dmul_rn(__dmul_rn(xl, xl), xl);
-        return __dsub_rn(__fma_rn(0.1, c, t), par(N * N + r));
+        return __dsub_rn(__fma_rn(0.1, c, t), par(N * LDA + r));
     }
     // The diagonal of J at x (the rest of J is A).
     __device__ __forceinline__ double diag(int i, double xi) const {
@@ -296,16 +301,25 @@ template <class Fam, int T, bool F, bool Mixed, bool PlainRef> struct WarpSolver
                                         double& jnorm) const {
         // ‖J‖_F as the column-major left fold: every lane folds all entries (the diagonal
         // arrives by broadcast, the rest is A)
-        double s = 0.0, mx = 0.0;
+        double s = 0.0;
         for (int k = 0; k < N; ++k) {
             const double dk = tm.bcast(diag_i, k);
             for (int i = 0; i < N; ++i) {
                 const double v = i == k ? dk : fam.A(i, k);
                 s = (i == 0 && k == 0) ? A::mul(v, v) : A::madd(v, v, s);
-                mx = (i == 0 && k == 0) ? jmax(fabs(v), 0.0) : jmax(mx, jmax(fabs(v), 0.0));
             }
         }
-        if (isfin(s) && s >= double(N * N) * kFloatmin) {
+        double mx = 0.0;
+        const bool direct = isfin(s) && s >= double(N * N) * kFloatmin;
+        if (!direct) {
+            // the scaled fallback of rnorm over the N*N entries
+            for (int k = 0; k < N; ++k) {
+                const double dk = tm.bcast(diag_i, k);
+                for (int i = 0; i < N; ++i)
+                    mx = jmax(mx, jmax(fabs(i == k ? dk : fam.A(i, k)), 0.0));
+            }
+        }
+        if (direct) {
             jnorm = sqrt(s);
         } else if (mx == 0.0 || !isfin(mx)) {
             jnorm = mx;

@@ -2,7 +2,7 @@
 #include "gsb_kernel_impl.cuh"
 
 namespace gsb {
-KernelEntry* warp_cubic24(bool fused, bool mixed, bool refine) {
+KernelEntry* warp_cubic24(bool fused, bool mixed, bool refine, int) {
     return pick_warp<WarpCubic<24>, 32>(fused, mixed, refine);
 }
 }  // namespace gsb

@@ -269,6 +269,34 @@ GSB_API int gsb_solve_batch_counts_noalloc(const GsbProblem* prob, const GsbMeth
                                            const int64_t* order, int32_t order_base,
                                            int64_t nsys, void* stream, GsbTally* tally);
 
+/* ─── ragged batches: systems of different sizes in one call ───────────────────────────────
+ *
+ * No counterpart in the reference, whose solve_batch! takes one size per call: a batch of
+ * cubic-affine systems (GSB_FAMILY_CUBIC_AFFINE) whose sizes n[s] are drawn from the set
+ * {2, 3, 4, 6, 8, 12, 16, 24, 32}, packed back to back: system s's iterate is X[x_off[s] ..
+ * x_off[s] + n[s]) and its parameter block (A column-major, then b) is P[p_off[s] .. p_off[s] +
+ * n[s]^2 + n[s]); its status is S[s] (72-byte status or 1-byte code, s_kind). The call buckets
+ * the systems by size on the device, then runs one persistent kernel per bucket, each taking
+ * CTA-sized chunks of its bucket from a device work queue; all of it is one CUDA graph, built
+ * on the first call with a given set of arguments and replayed after. `table` (nullable) gives,
+ * per bucket in the order of the sizes above, the threads per system (0: the default of the
+ * size; 1 up to n = 8, or 2, 4, 8 lanes for n = 6 and 8 under fused arithmetic; 16 or 32 lanes
+ * for n = 12 and 16; 32 for n = 24 and 32) and the persistent CTAs per SM (0: as many as fit).
+ * The call returns after the batch is solved; a size outside the set returns GSB_ERR_ARGUMENT
+ * (its systems are left untouched). All pointers are device pointers.
+ */
+#define GSB_UNEVEN_BUCKETS 9
+typedef struct {
+    int32_t threads_per_system;
+    int32_t ctas_per_sm;
+} GsbBucketConfig;
+
+GSB_API int gsb_uneven_sizes(int32_t* sizes_out /* GSB_UNEVEN_BUCKETS entries */);
+GSB_API int gsb_solve_batch_uneven(const GsbMethod* method, const GsbOptions* opt, double* X,
+                                   void* S, int32_t s_kind, const double* P, const int32_t* n,
+                                   const int64_t* x_off, const int64_t* p_off, int64_t nsys,
+                                   const GsbBucketConfig* table, void* stream, GsbTally* tally);
+
 #ifdef __cplusplus
 }
 #endif

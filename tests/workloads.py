@@ -74,3 +74,27 @@ def c2(nsys=524288, m=64):
     truth = np.stack([a[:, 0], b[:, 0], a[:, 1], b[:, 1], a[:, 2], b[:, 2]], axis=1)
     X0 = truth * (1.0 + g.uniform(-0.2, 0.2, (nsys, 6)))
     return np.ascontiguousarray(X0), np.ascontiguousarray(y), t
+
+
+C4_SIZES = (2, 3, 4, 6, 8, 12, 16, 24, 32)
+
+
+def c4(nsys=4194304):
+    """The ragged batch: sizes n from {2, 3, 4, 6, 8, 12, 16, 24, 32} with probability ∝ 1/n,
+    each system cubic-affine with A = (n+1) I + 0.5 N(0,1), b ~ U(-1, 1)^n, x0 = 0, packed back
+    to back. Returns (sizes (nsys,) int32, X0 (sum n,), P (sum n^2 + n,))."""
+    g = rng(4)
+    w = np.array([1.0 / n for n in C4_SIZES])
+    sizes = np.array(C4_SIZES, dtype=np.int32)[g.choice(len(C4_SIZES), nsys, p=w / w.sum())]
+    n64 = sizes.astype(np.int64)
+    p_len = n64 * n64 + n64
+    p_off = np.cumsum(p_len) - p_len
+    P = np.empty(int(p_len.sum()), dtype=np.float64)
+    for b, n in enumerate(C4_SIZES):
+        sel = np.flatnonzero(sizes == n)
+        if sel.size == 0:
+            continue
+        _, Pb = cubic_affine(n, sel.size, n + 1.0, 4, stream=b + 1)
+        idx = p_off[sel][:, None] + np.arange(n * n + n)[None, :]
+        P[idx] = Pb
+    return sizes, np.zeros(int(n64.sum()), dtype=np.float64), P

@@ -19,6 +19,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -40,8 +41,15 @@ def parse():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="gsb200", choices=["gsb200", "reference"])
     ap.add_argument("--nsys", type=int, default=NSYS)
-    ap.add_argument("--profile", choices=["plain", "mixed"], default=None,
-                    help="run `--warmup` + `--steps` solves of one form only (for ncu captures)")
+    ap.add_argument("--profile", choices=["plain", "mixed", "lm"], default=None,
+                    help="run `--warmup` + `--steps` solves of one form only (for ncu captures): "
+                         "the cubic-affine batch of size --n, or the exponential-sum fit (lm)")
+    ap.add_argument("--workload", choices=["c1", "c0", "c2", "c4"], default="c1",
+                    help="c1 (default): the n = 8 batch of the headline metric; c0: n = 3, "
+                         "65,536 systems; c2: the exponential-sum least-squares fit; c4: the "
+                         "ragged batch of sizes 2..32 (one GPU)")
+    ap.add_argument("--n", type=int, default=N_UNKNOWNS,
+                    help="cubic-affine size of a --profile run (A = 6I + ... at n = 8, else (n+1)I)")
     return ap.parse_args()
 
 
@@ -133,10 +141,10 @@ class Clocks:
     def __init__(self, index):
         self.index = index
         self.proc = None
-        self.path = os.path.join(ROOT, "_work", f"clocks_{os.getpid()}.csv")
+        fd, self.path = tempfile.mkstemp(prefix="gsb_clocks_", suffix=".csv")
+        os.close(fd)
 
     def __enter__(self):
-        os.makedirs(os.path.dirname(self.path), exist_ok=True)
         try:
             self.fh = open(self.path, "w")
             self.proc = subprocess.Popen(
@@ -237,6 +245,9 @@ def main():
         return
     if args.profile:
         run_profile(args)
+        return
+    if args.workload != "c1":
+        run_workload(args)
         return
 
     import torch
@@ -463,10 +474,21 @@ def run_profile(args):
 
     import gsb200 as G
 
-    X0_h, P_h = workload(0, args.nsys)
-    prob = G.NonlinearProblem(G.CubicAffine(N_UNKNOWNS))
-    plain, mixed = methods(G)
-    m = plain if args.profile == "plain" else mixed
+    if args.profile == "lm":
+        from workloads import c2
+
+        X0_h, P_h, t = c2(args.nsys)
+        prob = G.LeastSquaresProblem(G.ExpSum3(t))
+        m = G.Newton(linsolve=G.QRFactorization(), globalization=G.LevenbergMarquardt())
+    else:
+        from workloads import cubic_affine
+
+        n = args.n
+        X0_h, P_h = (workload(0, args.nsys) if n == N_UNKNOWNS
+                     else cubic_affine(n, args.nsys, n + 1.0, 4))
+        prob = G.NonlinearProblem(G.CubicAffine(n))
+        plain, mixed = methods(G)
+        m = plain if args.profile == "plain" else mixed
     X0 = torch.tensor(X0_h, device="cuda")
     P = G.PerSystem(torch.tensor(P_h, device="cuda"))
     X = torch.empty_like(X0)
@@ -478,6 +500,281 @@ def run_profile(args):
     st = G.statuses(S)
     print(json.dumps({"profile": args.profile, "nsys": args.nsys,
                       "codes": np.bincount(st["code"], minlength=6).tolist()}))
+
+
+# ─── the other configurations, one GPU: c0 (n = 3), c2 (least squares), c4 (ragged) ─────────
+
+
+def lm_flops_per_system(m, n, iterations, failures):
+    """Operations of the Levenberg–Marquardt solve of the exponential-sum fit (an `exp` counts
+    one), from the oracle's per-system counts: one Jacobian pass per step (rows by the dual
+    rules, J'F, ‖J‖, the stacked Givens reduction) and one trial per step or rejected trial (the
+    damped triangle, back substitution, the predicted reduction, a residual evaluation)."""
+    row_f = 9 + 3                                     # residual row with its three exps
+    rot = 6 * n + 6 * n * (n - 1) // 2 + 6 * n         # one row rotated into the triangle
+    jpass = m * (row_f + 6 + 4 * n) + (m - n) * rot + n * rot
+    trial = n * rot // 2 + n * n + 4 * n + m * (row_f + 2)
+    return iterations * jpass + (iterations + failures) * trial
+
+
+def _events_ms(fn, steps, warmup, stream):
+    import torch
+
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def _cpu_sample(solve_sample, sample, label):
+    """Time the oracle on `sample` systems until about 10 s have passed."""
+    from oracle import oracle_py as O
+
+    nt = O.max_threads()
+    reps, t_tot = 0, 0.0
+    while t_tot < 10.0 and reps < 40:
+        t0 = time.perf_counter()
+        solve_sample(nt)
+        t_tot += time.perf_counter() - t0
+        reps += 1
+    return {"value": sample * reps / t_tot, "unit": "systems/s", "cores": nt, "kind": "port",
+            "sample": f"{reps} x {sample} systems of {label}, {nt} threads, {t_tot:.1f} s"}
+
+
+def _roof(bytes_total, flops, kms, peaks, hbm_peak, hbm_src, kernel):
+    t_bytes = bytes_total / (hbm_peak * 1e9)
+    t_flops = flops / (peaks["fp64"] * 1e12)
+    gbs = bytes_total / (kms * 1e-3) / 1e9
+    tf = flops / (kms * 1e-3) / 1e12
+    if t_bytes >= t_flops:
+        r = {"bound": "hbm", "achieved": gbs, "peak": hbm_peak, "unit": "GB/s",
+             "frac": gbs / hbm_peak, "peak_source": f"{hbm_src} (MEASURED_PEAKS.json hbm_gbs)"}
+    else:
+        r = {"bound": "fp64", "achieved": tf, "peak": peaks["fp64"], "unit": "TFLOP/s",
+             "frac": tf / peaks["fp64"], "peak_source": "measured (FP64 FMA probe, libgsbpeak)"}
+    r.update(traffic=None, kernel=kernel, kernel_ms=kms, fp64_frac=tf / peaks["fp64"],
+             hbm_frac=gbs / hbm_peak, flops_per_launch=flops, bytes_per_launch=bytes_total)
+    return r
+
+
+def run_workload(args):
+    import torch
+
+    import gsb200 as G
+    from oracle import oracle_py as O
+
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.current_stream(dev)
+    opts = options(G)
+    hbm_peak, hbm_src = measured_peaks()
+    peaks = fp_peaks()
+    forms = {}
+
+    if args.workload in ("c0", "c2"):
+        if args.workload == "c0":
+            from workloads import c0
+
+            nsys = args.nsys if args.nsys != NSYS else 65536
+            X0_h, P_h = c0(nsys)
+            prob = G.NonlinearProblem(G.CubicAffine(3))
+            method = G.Newton(globalization=G.Backtracking())
+            workload = (f"cubic-affine n=3, {nsys} systems, A = 4I + 0.5 N(0,1), Newton + LU + "
+                        "Backtracking FP64, f_abstol 1e-12, max_iterations 50")
+            kernel = "newton_kernel<CubicAffine<3>, fused, FP64>"
+        else:
+            from workloads import c2
+
+            nsys = args.nsys if args.nsys != NSYS else 524288
+            X0_h, P_h, t = c2(nsys)
+            prob = G.LeastSquaresProblem(G.ExpSum3(t))
+            method = G.Newton(linsolve=G.QRFactorization(), globalization=G.LevenbergMarquardt())
+            workload = (f"exponential-sum least squares m=64 n=6, {nsys} systems, "
+                        "LevenbergMarquardt (stacked QR), FP64, max_iterations 50")
+            kernel = "lm_kernel<ExpSum3<64>, fused>"
+        X0 = torch.tensor(X0_h, device=dev)
+        P = torch.tensor(P_h, device=dev)
+        X = torch.empty_like(X0)
+        S = G.status_buffer(nsys)
+        ps = G.PerSystem(P)
+
+        def step():
+            X.copy_(X0)
+            G.solve_batch(X, S, prob, method, ps, options=opts)
+
+        # correctness against the oracle (untimed), on the whole batch for c0 and on a sample
+        # of 65,536 systems for c2 (codes equal and |F| within the fit's 1e-10 envelope)
+        step()
+        st = G.statuses(S)
+        x = X.cpu().numpy()
+        ns = nsys if args.workload == "c0" else min(nsys, 65536)
+        xo, so = O.solve_batch(prob, method, X0_h[:ns].copy(), P_h[:ns], opts)
+        if args.workload == "c0":
+            ok = (st["code"][:ns] == so["code"]) & (rel_err(x[:ns], xo) <= REL_TOL)
+            flops = float(np.sum(flops_per_system(3, so["iterations"].astype(np.int64),
+                                                  1 + _trials(so))))
+            bytes_total = bytes_per_system(3) * nsys
+        else:
+            fr = np.abs(st["fnorm"][:ns] - so["fnorm"]) / np.maximum(so["fnorm"], 1e-300)
+            ok = (st["code"][:ns] == so["code"]) & (fr <= np.where(so["code"] == 0, 1e-10, 1e-9))
+            flops = float(np.mean(lm_flops_per_system(
+                64, 6, st["iterations"].astype(np.int64), st["step_failures"].astype(np.int64))))
+            flops *= nsys
+            bytes_total = (512 + 48 + 48 + 72) * nsys
+        solved_frac = float(np.mean(ok))
+        with Clocks(0) as clk:
+            ms = _events_ms(step, args.steps, args.warmup, stream)
+        clocks = clk.summary()
+        value = solved_frac * nsys / (ms * 1e-3)
+        # the solve alone: the step minus the copy of the start iterates
+        kms = ms - _events_ms(lambda: X.copy_(X0), 20, 2, stream)
+        # end to end: pinned host inputs in, solutions and statuses out, every step
+        x_pin = torch.from_numpy(X0_h).pin_memory()
+        p_pin = torch.from_numpy(P_h).pin_memory()
+        x_out = torch.empty_like(x_pin).pin_memory()
+        s_out = torch.empty((nsys, 72), dtype=torch.uint8).pin_memory()
+        Xe, Pe = torch.empty_like(X0), torch.empty_like(P)
+
+        def e2e():
+            Xe.copy_(x_pin, non_blocking=True)
+            Pe.copy_(p_pin, non_blocking=True)
+            G.solve_batch(Xe, S, prob, method, G.PerSystem(Pe), options=opts)
+            x_out.copy_(Xe, non_blocking=True)
+            s_out.copy_(S, non_blocking=True)
+
+        ms_e2e = _events_ms(e2e, max(1, args.steps // 2), 1, stream)
+        h2d, d2h = X0_h.nbytes + P_h.nbytes, X0_h.nbytes + nsys * 72
+        sample = min(nsys, 65536 if args.workload == "c0" else 8192)
+        cpu = _cpu_sample(lambda nt: O.solve_batch(prob, method, X0_h[:sample].copy(),
+                                                   P_h[:sample], opts, nthreads=nt),
+                          sample, args.workload)
+        forms["fp64"] = {"systems_per_s": value, "ms_per_step": ms, "solved_fraction": solved_frac,
+                         "oracle_checked_systems": ns}
+        launches = args.steps
+        chosen = "fp64"
+    else:
+        from workloads import c4
+
+        nsys = args.nsys if args.nsys != NSYS else 4194304
+        sizes_h, X0_h, P_h = c4(nsys)
+        sizes = torch.tensor(sizes_h, dtype=torch.int32, device=dev)
+        X0 = torch.tensor(X0_h, device=dev)
+        P = torch.tensor(P_h, device=dev)
+        X = torch.empty_like(X0)
+        S = G.status_buffer(nsys)
+        x_off, p_off = G.ragged_offsets(sizes)
+        plain, mixed = methods(G)
+        # the oracle, bucket by bucket (untimed)
+        n64 = sizes_h.astype(np.int64)
+        xo_all = np.empty_like(X0_h)
+        so_all = np.zeros(nsys, dtype=G.SOLVER_STATUS_DTYPE)
+        xoff_h, poff_h = x_off.cpu().numpy(), p_off.cpu().numpy()
+        flops = 0.0
+        for n in (2, 3, 4, 6, 8, 12, 16, 24, 32):
+            sel = np.flatnonzero(sizes_h == n)
+            xi = xoff_h[sel][:, None] + np.arange(n)[None, :]
+            pi = poff_h[sel][:, None] + np.arange(n * n + n)[None, :]
+            xo, so = O.solve_batch(G.NonlinearProblem(G.CubicAffine(n)), plain, X0_h[xi].copy(),
+                                   P_h[pi], opts)
+            xo_all[xi] = xo
+            so_all[sel] = so
+            flops += float(np.sum(flops_per_system(n, so["iterations"].astype(np.int64),
+                                                   1 + _trials(so))))
+        bytes_total = float(np.sum(8 * n64 + 8 * (n64 * n64 + n64) + 8 * n64 + 72 + 4 + 16))
+        tables = {"plain_fp64": None, "fp32_lu_refinement": None}
+        for name, m in (("plain_fp64", plain), ("fp32_lu_refinement", mixed)):
+            tables[name], _ = G.tune.autotune_uneven(m, options=opts, sample=16384, reps=2)
+
+        def solver(m, table):
+            def step():
+                X.copy_(X0)
+                G.solve_batch_uneven(X, S, sizes, P, m, x_off=x_off, p_off=p_off, table=table,
+                                     options=opts)
+            return step
+
+        with Clocks(0) as clk:
+            for name, m in (("plain_fp64", plain), ("fp32_lu_refinement", mixed)):
+                step = solver(m, tables[name])
+                ms = _events_ms(step, args.steps, args.warmup, stream)
+                step()
+                st = G.statuses(S)
+                x = X.cpu().numpy()
+                ok = st["code"] == so_all["code"]
+                err = np.zeros(nsys)
+                for n in (2, 3, 4, 6, 8, 12, 16, 24, 32):
+                    sel = np.flatnonzero(sizes_h == n)
+                    xi = xoff_h[sel][:, None] + np.arange(n)[None, :]
+                    err[sel] = rel_err(x[xi], xo_all[xi])
+                ok &= err <= REL_TOL
+                forms[name] = {"systems_per_s": float(np.sum(ok)) / (ms * 1e-3), "ms_per_step": ms,
+                               "solved": int(np.sum(ok)), "fp64_oracle_max_rel_err": float(err.max()),
+                               "table": tables[name]}
+        clocks = clk.summary()
+        chosen = max(forms, key=lambda k: forms[k]["systems_per_s"])
+        value = forms[chosen]["systems_per_s"]
+        ms = forms[chosen]["ms_per_step"]
+        forms["chosen_over_plain"] = value / forms["plain_fp64"]["systems_per_s"]
+        m_ch = mixed if chosen == "fp32_lu_refinement" else plain
+        kms = ms - _events_ms(lambda: X.copy_(X0), 20, 2, stream)
+        kernel = "bucketing + 9 persistent bucket kernels (one CUDA graph)"
+        x_pin = torch.from_numpy(X0_h).pin_memory()
+        p_pin = torch.from_numpy(P_h).pin_memory()
+        n_pin = torch.from_numpy(sizes_h).pin_memory()
+        x_out = torch.empty_like(x_pin).pin_memory()
+        s_out = torch.empty((nsys, 72), dtype=torch.uint8).pin_memory()
+        Xe, Pe = torch.empty_like(X0), torch.empty_like(P)
+        ne = torch.empty_like(sizes)
+
+        def e2e():
+            Xe.copy_(x_pin, non_blocking=True)
+            Pe.copy_(p_pin, non_blocking=True)
+            ne.copy_(n_pin, non_blocking=True)
+            G.solve_batch_uneven(Xe, S, ne, Pe, m_ch, table=tables[chosen], options=opts)
+            x_out.copy_(Xe, non_blocking=True)
+            s_out.copy_(S, non_blocking=True)
+
+        ms_e2e = _events_ms(e2e, max(1, args.steps // 2), 1, stream)
+        h2d, d2h = X0_h.nbytes + P_h.nbytes + sizes_h.nbytes, X0_h.nbytes + nsys * 72
+        sample = 131072
+
+        def cpu_solve(nt):
+            for n in (2, 3, 4, 6, 8, 12, 16, 24, 32):
+                sel = np.flatnonzero(sizes_h[:sample] == n)
+                xi = xoff_h[sel][:, None] + np.arange(n)[None, :]
+                pi = poff_h[sel][:, None] + np.arange(n * n + n)[None, :]
+                O.solve_batch(G.NonlinearProblem(G.CubicAffine(n)), plain, X0_h[xi].copy(),
+                              P_h[pi], opts, nthreads=nt)
+
+        cpu = _cpu_sample(cpu_solve, sample, "the ragged batch, plain FP64")
+        workload = (f"ragged cubic-affine batch, {nsys} systems, n in {{2,...,32}} with P(n) ∝ 1/n, "
+                    "A = (n+1)I + 0.5 N(0,1), Newton + LU + Backtracking, autotuned persistent "
+                    "bucket kernels in one CUDA graph")
+        launches = args.steps * 13
+    line = {
+        "metric": METRIC, "value": value, "unit": "systems/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded; the configuration's shapes and distributions)",
+        "config": {"workload": workload, "chosen_form": chosen, "global_batch": nsys,
+                   "parallelism": "one GPU",
+                   "l2": f"inputs of {bytes_total / 1e6:.0f} MB per step exceed the 126 MB L2"
+                   if bytes_total > 126e6 else "inputs fit in L2; a step rewrites X from X0"},
+        "forms": forms,
+        "e2e": {"value": value * ms / ms_e2e, "unit": "systems/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h), "ms_per_step": ms_e2e},
+        "gpu_launches": launches,
+        "roofline": _roof(bytes_total, flops, kms, peaks, hbm_peak, hbm_src, kernel),
+        "cpu_baseline": cpu,
+        "clocks": clocks,
+    }
+    print(json.dumps(line), flush=True)
 
 
 def _trials(so):

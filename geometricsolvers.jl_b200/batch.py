@@ -173,6 +173,9 @@ def batch_summary(S, stream=None) -> BatchSummary:
                         int(out.max_iterations), int(out.total_iterations))
 
 
+_ragged_cache = {}
+
+
 def ragged_offsets(sizes):
     """The offsets (in doubles) of each system's iterate and cubic-affine parameter block in the
     packed X and P of a ragged batch: exclusive prefix sums of n and n^2 + n."""
@@ -205,9 +208,22 @@ def solve_batch_uneven(X, S, sizes, P, method, *, x_off=None, p_off=None, table=
     nsys = sizes.numel()
     n_dev = sizes.to(device=X.device, dtype=torch.int32).contiguous()
     if x_off is None or p_off is None:
+        # The sizes and offsets go into buffers kept per batch length and device, rewritten on
+        # every call, so that repeated calls pass the same pointers and replay one graph.
+        key = (nsys, str(X.device))
+        if _ragged_cache.get("key") != key:
+            _ragged_cache.clear()
+            _ragged_cache.update(key=key,
+                                 n=torch.empty(nsys, dtype=torch.int32, device=X.device),
+                                 x=torch.empty(nsys, dtype=torch.int64, device=X.device),
+                                 p=torch.empty(nsys, dtype=torch.int64, device=X.device))
+        _ragged_cache["n"].copy_(n_dev)
         xo, po = ragged_offsets(n_dev)
-        x_off = xo if x_off is None else x_off
-        p_off = po if p_off is None else p_off
+        _ragged_cache["x"].copy_(xo)
+        _ragged_cache["p"].copy_(po)
+        n_dev = _ragged_cache["n"]
+        x_off = _ragged_cache["x"] if x_off is None else x_off
+        p_off = _ragged_cache["p"] if p_off is None else p_off
     x_off = torch.as_tensor(x_off).to(device=X.device, dtype=torch.int64).contiguous()
     p_off = torch.as_tensor(p_off).to(device=X.device, dtype=torch.int64).contiguous()
     if x_off.numel() != nsys or p_off.numel() != nsys:

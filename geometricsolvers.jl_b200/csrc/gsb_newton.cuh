@@ -77,6 +77,10 @@ __device__ __forceinline__ void cswap(int r, int p, float& x, float& y) {
 // factor_matrix (src/linear/factors.jl:802-811): TF = T divides by 2^e only for e < 0; another
 // TF divides for every e != 0, in T, then rounds to TF.
 template <bool F, int N, class TF> struct LUFactor {
+    // Under fused arithmetic the Float32 factor of the mixed step (whose result the Float64
+    // refinement corrects) divides by multiplying with reciprocals: of each pivot, and of the
+    // scale s of its right-hand sides.
+    static constexpr bool kRecip = F && sizeof(TF) == sizeof(float);
     TF a[N * N];
     int ipiv[N];
     int info;
@@ -140,6 +144,18 @@ template <bool F, int N, class TF> struct LUFactor {
             TF akk = a[k + k * N];
             if (akk == TF(0)) {
                 if (info == 0) info = k + 1;
+            } else if constexpr (kRecip) {
+                // the fused Float32 factor: one reciprocal per pivot, kept in place of the
+                // pivot for the back substitution
+                const TF r = TF(1) / akk;
+                a[k + k * N] = r;
+#pragma unroll
+                for (int i = k + 1; i < N; ++i) a[i + k * N] = a[i + k * N] * r;
+#pragma unroll
+                for (int j = k + 1; j < N; ++j)
+#pragma unroll
+                    for (int i = k + 1; i < N; ++i)
+                        a[i + j * N] = Arith<F>::msub(a[i + k * N], a[k + j * N], a[i + j * N]);
             } else {
 #pragma unroll
                 for (int i = k + 1; i < N; ++i) a[i + k * N] = a[i + k * N] / akk;
@@ -170,7 +186,7 @@ template <bool F, int N, class TF> struct LUFactor {
         }
 #pragma unroll
         for (int k = N - 1; k >= 0; --k) {
-            TF xk = x[k] / a[k + k * N];
+            TF xk = kRecip ? x[k] * a[k + k * N] : x[k] / a[k + k * N];
             x[k] = xk;
 #pragma unroll
             for (int i = 0; i < k; ++i) x[i] = Arith<F>::msub(a[i + k * N], xk, x[i]);
@@ -199,7 +215,7 @@ template <bool F, int N, class TF> struct LUFactor {
             }
             TF x[N];
 #pragma unroll
-            for (int i = 0; i < N; ++i) x[i] = TF(__ddiv_rn(r[i], s));
+            for (int i = 0; i < N; ++i) x[i] = TF(kRecip ? __dmul_rn(r[i], __drcp_rn(s)) : __ddiv_rn(r[i], s));
             backsolve(x);
             int ex = 0;
             double frac = isfin(s) ? frexp(s, &ex) : s;

@@ -131,6 +131,8 @@ template <int N, int T, bool F> struct WarpVec {
 // pivot of column k in `piv`.
 template <int N, int T, bool F, class TF> struct WarpLU {
     static constexpr int LD = warp_ld(N);
+    // the fused Float32 factor divides by multiplying with reciprocals (see LUFactor)
+    static constexpr bool kRecip = F && sizeof(TF) == sizeof(float);
     using A = Arith<F>;
     TF* a;
     int piv;
@@ -210,10 +212,15 @@ template <int N, int T, bool F, class TF> struct WarpLU {
             const TF akk = at(k, k);
             if (akk == TF(0)) {
                 if (info == 0) info = k + 1;
-            } else if (lane > k && lane < N) {
-                const TF l = at(lane, k) / akk;
-                at(lane, k) = l;
-                for (int j = k + 1; j < N; ++j) at(lane, j) = A::msub(l, at(k, j), at(lane, j));
+            } else {
+                const TF rk = kRecip ? TF(1) / akk : TF(0);
+                if (lane > k && lane < N) {
+                    const TF l = kRecip ? at(lane, k) * rk : at(lane, k) / akk;
+                    at(lane, k) = l;
+                    for (int j = k + 1; j < N; ++j) at(lane, j) = A::msub(l, at(k, j), at(lane, j));
+                }
+                // the reciprocal replaces the pivot for the back substitution
+                if (kRecip && lane == k) at(k, k) = rk;
             }
             __syncwarp(tm.mask);
         }
@@ -236,7 +243,7 @@ template <int N, int T, bool F, class TF> struct WarpLU {
             if (lane > k && lane < N) x = A::msub(at(lane, k), xk, x);
         }
         for (int k = N - 1; k >= 0; --k) {
-            if (lane == k) x = x / at(k, k);
+            if (lane == k) x = kRecip ? x * at(k, k) : x / at(k, k);
             const TF xk = tm.bcast(x, k);
             if (lane < k) x = A::msub(at(lane, k), xk, x);
         }
@@ -259,7 +266,7 @@ template <int N, int T, bool F, class TF> struct WarpLU {
         } else {
             const double s = wv.maxabs(r);
             if (s == 0.0) return 0.0;
-            TF x = TF(__ddiv_rn(r, s));
+            TF x = TF(kRecip ? __dmul_rn(r, __drcp_rn(s)) : __ddiv_rn(r, s));
             backsolve(tm, x);
             int ex = 0;
             double frac = isfin(s) ? frexp(s, &ex) : s;

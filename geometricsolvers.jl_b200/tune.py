@@ -55,7 +55,8 @@ def _time(solve, reps):
 
 def autotune_uneven(method, options=None, sample=16384, reps=3, generator=None, sizes=None,
                     verbose=False):
-    """Returns (table, timings): the table for ``solve_batch_uneven`` (nine (threads_per_system,
+    """`sample` systems of size 32 per timing, proportionally more of the smaller sizes (up to
+    262,144). Returns (table, timings): the table for ``solve_batch_uneven`` (nine (threads_per_system,
     ctas_per_sm) pairs) and, per size, the milliseconds of every configuration tried."""
     import torch
 
@@ -67,9 +68,11 @@ def autotune_uneven(method, options=None, sample=16384, reps=3, generator=None, 
     for b, n in enumerate(UNEVEN_SIZES):
         if sizes is not None and n not in sizes:
             continue
-        X0, P = (generator or synthetic_bucket)(n, sample)
+        # small systems take more samples, so that a timing is not a launch latency
+        count = min(262144, sample * max(1, 32 // n))
+        X0, P = (generator or synthetic_bucket)(n, count)
         X = torch.empty_like(X0)
-        nv = torch.full((sample,), n, dtype=torch.int32, device=X0.device)
+        nv = torch.full((count,), n, dtype=torch.int32, device=X0.device)
         best, best_ms, tried = None, float("inf"), {}
         for T in CANDIDATE_THREADS[n]:
             if T > 1 and n <= 8 and not fused:

@@ -339,7 +339,7 @@ __global__ void __launch_bounds__(kThreads) warp_kernel(GsbMethod m, GsbOptions 
         const int64_t idx = r.order ? r.order[i] - L.order_base : i;
         Team<T> tm;
         const int lane = tm.lane;
-        Fam fam{sys};
+        Fam fam{sys, L.shared};
         double* xb = x_block(L, idx, N);
         double xl = 0.0;
         if (lane < N) xl = L.x_layout == GSB_SOA ? L.X[(int64_t)lane * L.nsys + idx] : xb[lane];

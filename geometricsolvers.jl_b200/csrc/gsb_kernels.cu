@@ -179,6 +179,7 @@ KernelEntry* warp_cubic12(bool fused, bool mixed, bool refine, int T);
 KernelEntry* warp_cubic16(bool fused, bool mixed, bool refine, int T);
 KernelEntry* warp_cubic24(bool fused, bool mixed, bool refine, int T);
 KernelEntry* warp_cubic32(bool fused, bool mixed, bool refine, int T);
+KernelEntry* warp_irk(bool fused, bool mixed, bool refine, int T);
 }  // namespace gsb
 
 namespace {
@@ -206,6 +207,10 @@ KernelEntry* select_kernel(const GsbProblem* prob, bool fused, bool mixed, bool 
         case 32: return warp_cubic32(fused, mixed, refine, T);
         default: return nullptr;
         }
+    }
+    if (prob->family == GSB_FAMILY_IRK3_HENON_HEILES) {
+        if (T == 0) T = 16;
+        return (T == 16 || T == 32) ? warp_irk(fused, mixed, refine, T) : nullptr;
     }
     if (T == 0) T = fused ? tuned_team(prob, mixed) : 1;
     if (T != 1) {
@@ -328,6 +333,8 @@ int launch_solve(const GsbProblem* prob, const GsbMethod* method, const GsbOptio
                            "LevenbergMarquardt batch kernel only for least-squares families");
         if (method->linsolve != GSB_LU)
             return set_err(GSB_ERR_UNSUPPORTED, "QRFactorization batch kernel not in this build");
+        if (prob->family == GSB_FAMILY_IRK3_HENON_HEILES && !prob->shared)
+            return set_err(GSB_ERR_ARGUMENT, "the step h and the tableau A are missing");
         ke = select_kernel(prob, fused, mixed, method->refinement == GSB_REFINEMENT,
                            method->threads_per_system);
     }
@@ -472,6 +479,8 @@ int gsb_solve_batch(const GsbProblem* prob, const GsbMethod* method, const GsbOp
                            "LevenbergMarquardt batch kernel only for least-squares families");
         if (method->linsolve != GSB_LU)
             return set_err(GSB_ERR_UNSUPPORTED, "QRFactorization batch kernel not in this build");
+        if (prob->family == GSB_FAMILY_IRK3_HENON_HEILES && !prob->shared)
+            return set_err(GSB_ERR_ARGUMENT, "the step h and the tableau A are missing");
         ke = select_kernel(prob, fused, mixed, method->refinement == GSB_REFINEMENT,
                            method->threads_per_system);
     }

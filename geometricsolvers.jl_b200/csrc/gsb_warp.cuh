@@ -33,7 +33,12 @@ __host__ __device__ constexpr int warp_ld(int n) { return (n % 2 == 1) ? n : n +
 // reading down a column, fall in distinct bank slots), then b.
 template <int N_> struct WarpCubic {
     static constexpr int N = N_, NP = N_ * N_ + N_, LDA = warp_ld(N_), SP = N_ * LDA + N_;
+    static constexpr bool kDiagState = true;  // J = A except a diagonal held by the lanes
     const double* p;
+    const double* shared;  // unused: the family has no batch-wide constants
+    struct JState {
+        double d;  // J_ii of the lane's row i
+    };
     // place of parameter k (A column-major, then b) in the shared-memory block
     __host__ __device__ static constexpr int place(int k) {
         return k < N * N ? (k % N) + (k / N) * LDA : N * LDA + (k - N * N);
@@ -60,6 +65,23 @@ template <int N_> struct WarpCubic {
     __device__ __forceinline__ double J(int i, int k, double diag_i) const {
         return i == k ? diag_i : A(i, k);
     }
+    // the Jacobian at x: the lane's diagonal entry
+    template <int T>
+    __device__ __forceinline__ JState jacobian(const Team<T>& tm, double xl) const {
+        return {diag(tm.lane, xl)};
+    }
+    // J_ik where i == k only for the lane's own row i (jmul, the factor, column folds)
+    __device__ __forceinline__ double Jent(const JState& js, int i, int k) const {
+        return i == k ? js.d : A(i, k);
+    }
+    // J_ik for a fold over all entries; dk = J_kk, broadcast by col_diag
+    template <int T>
+    __device__ __forceinline__ double col_diag(const Team<T>& tm, const JState& js, int k) const {
+        return tm.bcast(js.d, k);
+    }
+    __device__ __forceinline__ double Jall(const JState&, int i, int k, double dk) const {
+        return i == k ? dk : A(i, k);
+    }
     template <int T>
     __device__ __forceinline__ double jvp(const Team<T>& tm, int i, double xi, double vl) const {
         const int r = i < N ? i : N - 1;
@@ -70,6 +92,118 @@ template <int N_> struct WarpCubic {
         const double x2p = __dadd_rn(xv, xv);
         const double cp = __dadd_rn(__dmul_rn(x2p, xi), __dmul_rn(vl, __dmul_rn(xi, xi)));
         return __fma_rn(0.1, cp, t);
+    }
+};
+
+// The Gauss–Legendre 3-stage equations of the Hénon–Heiles field in row form:
+// G(Z) = Z - h (A ⊗ I) f(y + Z), Z = (Z_1, Z_2, Z_3) stacked stage increments, row r = 4 i + k.
+// The operations and their order are those of the stage residual (test/helpers/
+// stage_problems.jl:205-222, restated in the oracle), each product and sum rounded alone. The
+// Jacobian is the forward-mode one (src/ad/forwarddiff_static.jl:50-65), written out for this
+// field: row r's partials are exact dual-rule values, and a lane computes its own row into the
+// held Jacobian in shared memory. `p` holds the state y (4 doubles), then the held Jacobian
+// (12 x LD); `shared` (device memory) holds h and the tableau A column-major.
+struct WarpIrk {
+    static constexpr int N = 12, NP = 4, LD = warp_ld(12), SP = 4 + 12 * LD;
+    static constexpr bool kDiagState = false;
+    const double* p;
+    const double* shared;
+    struct JState {
+        const double* J;  // the held Jacobian, row i at J + i * LD
+    };
+    __host__ __device__ static constexpr int place(int k) { return k; }
+    __device__ __forceinline__ double y(int k) const { return lds(smem_addr(p) + 8u * k); }
+    __device__ __forceinline__ double coef(int i, int j) const {
+        return __dmul_rn(__ldg(shared), __ldg(shared + 1 + i + 3 * j));  // h * A_ij
+    }
+
+    // one field component k at the stage value Y
+    __device__ __forceinline__ static double field(int k, double Y0, double Y1, double Y2, double Y3) {
+        if (k == 0) return Y2;
+        if (k == 1) return Y3;
+        if (k == 2) return __dsub_rn(-Y0, __dmul_rn(2.0, __dmul_rn(Y0, Y1)));
+        return __dadd_rn(__dsub_rn(-Y1, __dmul_rn(Y0, Y0)), __dmul_rn(Y1, Y1));
+    }
+
+    template <int T>
+    __device__ __forceinline__ double F(const Team<T>& tm, int r, double zl) const {
+        const int rr = r < N ? r : N - 1;
+        const int i = rr / 4, kk = rr % 4;
+        double out = zl;
+        for (int j = 0; j < 3; ++j) {
+            const double Y0 = __dadd_rn(y(0), tm.bcast(zl, 4 * j));
+            const double Y1 = __dadd_rn(y(1), tm.bcast(zl, 4 * j + 1));
+            const double Y2 = __dadd_rn(y(2), tm.bcast(zl, 4 * j + 2));
+            const double Y3 = __dadd_rn(y(3), tm.bcast(zl, 4 * j + 3));
+            out = __dsub_rn(out, __dmul_rn(coef(i, j), field(kk, Y0, Y1, Y2, Y3)));
+        }
+        return out;
+    }
+
+    // The lane's row of J into the held Jacobian: J_rc = [c == r] - a_ij df_k/dY_m for c = 4 j + m.
+    template <int T>
+    __device__ __forceinline__ JState jacobian(const Team<T>& tm, double zl) const {
+        double* J = const_cast<double*>(p) + 4;
+        const int r = tm.lane;
+        const int i = (r < N ? r : N - 1) / 4, kk = (r < N ? r : N - 1) % 4;
+        for (int j = 0; j < 3; ++j) {
+            const double Y0 = __dadd_rn(y(0), tm.bcast(zl, 4 * j));
+            const double Y1 = __dadd_rn(y(1), tm.bcast(zl, 4 * j + 1));
+            const double a = coef(i, j);
+            // df_kk / dY_m by the dual rules
+            double fp[4] = {0.0, 0.0, 0.0, 0.0};
+            if (kk == 0) fp[2] = 1.0;
+            else if (kk == 1) fp[3] = 1.0;
+            else if (kk == 2) {
+                fp[0] = __dsub_rn(-1.0, __dmul_rn(2.0, Y1));
+                fp[1] = -__dmul_rn(2.0, Y0);
+            } else {
+                fp[0] = -__dadd_rn(Y0, Y0);
+                fp[1] = __dadd_rn(-1.0, __dadd_rn(Y1, Y1));
+            }
+            if (r < N) {
+#pragma unroll
+                for (int m = 0; m < 4; ++m) {
+                    const int c = 4 * j + m;
+                    const double t = __dmul_rn(a, fp[m]);
+                    J[r * LD + c] = c == r ? __dsub_rn(1.0, t) : -t;
+                }
+            }
+        }
+        __syncwarp(tm.mask);
+        return {J};
+    }
+    __device__ __forceinline__ double Jent(const JState& js, int i, int k) const {
+        return lds(smem_addr(js.J) + 8u * (i * LD + k));
+    }
+    template <int T>
+    __device__ __forceinline__ double col_diag(const Team<T>&, const JState&, int) const { return 0.0; }
+    __device__ __forceinline__ double Jall(const JState& js, int i, int k, double) const {
+        return Jent(js, i, k);
+    }
+
+    // Row r of J(Z) v by the one-partial dual rules.
+    template <int T>
+    __device__ __forceinline__ double jvp(const Team<T>& tm, int r, double zl, double vl) const {
+        const int rr = r < N ? r : N - 1;
+        const int i = rr / 4, kk = rr % 4;
+        double out = vl;
+        for (int j = 0; j < 3; ++j) {
+            const double Y0 = __dadd_rn(y(0), tm.bcast(zl, 4 * j));
+            const double Y1 = __dadd_rn(y(1), tm.bcast(zl, 4 * j + 1));
+            const double p0 = tm.bcast(vl, 4 * j), p1 = tm.bcast(vl, 4 * j + 1);
+            const double p2 = tm.bcast(vl, 4 * j + 2), p3 = tm.bcast(vl, 4 * j + 3);
+            double fp;
+            if (kk == 0) fp = p2;
+            else if (kk == 1) fp = p3;
+            else if (kk == 2)
+                fp = __dsub_rn(-p0, __dmul_rn(2.0, __dadd_rn(__dmul_rn(p0, Y1), __dmul_rn(p1, Y0))));
+            else
+                fp = __dadd_rn(__dsub_rn(-p1, __dadd_rn(__dmul_rn(p0, Y0), __dmul_rn(p0, Y0))),
+                               __dadd_rn(__dmul_rn(p1, Y1), __dmul_rn(p1, Y1)));
+            out = __dsub_rn(out, __dmul_rn(coef(i, j), fp));
+        }
+        return out;
     }
 };
 
@@ -143,7 +277,7 @@ template <int N, int T, bool F, class TF> struct WarpLU {
     // J into the factor (row `lane` from the lane's row values), factor_matrix's scaling, then
     // the elimination (lu.jl:24-64).
     template <class Fam>
-    __device__ void factor(const Team<T>& tm, const Fam& fam, double diag_i) {
+    __device__ void factor(const Team<T>& tm, const Fam& fam, const typename Fam::JState& js) {
         const int lane = tm.lane;
         const bool mine = lane < N;
         constexpr bool same = sizeof(TF) == sizeof(double);
@@ -151,7 +285,7 @@ template <int N, int T, bool F, class TF> struct WarpLU {
         if (mine)
             for (int k = 0; k < N; ++k) {
                 const unsigned long long b =
-                    FBits<double>::bits(fam.J(lane, k, diag_i)) & ~FBits<double>::sign_mask;
+                    FBits<double>::bits(fam.Jent(js, lane, k)) & ~FBits<double>::sign_mask;
                 mb = b > mb ? b : mb;
             }
         const double mm = FBits<double>::from(tm.umax(mb));
@@ -164,14 +298,14 @@ template <int N, int T, bool F, class TF> struct WarpLU {
             e = ex < 0 ? ex : 0;
             if (mine)
                 for (int k = 0; k < N; ++k) {
-                    const double v = fam.J(lane, k, diag_i);
+                    const double v = fam.Jent(js, lane, k);
                     at(lane, k) = e < 0 ? scale2_in(v, -e) : v;  // -e in [1, 1023]
                 }
         } else {
             e = (isfin(mm) && mm != 0.0) ? max(-1023, min(1023, jexponent(mm))) : 0;
             if (mine)
                 for (int k = 0; k < N; ++k) {
-                    const double v = fam.J(lane, k, diag_i);
+                    const double v = fam.Jent(js, lane, k);
                     at(lane, k) = TF(e == 0 ? v : scale2_in(v, -e));  // -e in [-1023, 1023]
                 }
         }
@@ -281,6 +415,7 @@ template <int N, int T, bool F, class TF> struct WarpLU {
 template <class Fam, int T, bool F, bool Mixed, bool PlainRef> struct WarpSolver {
     static constexpr int N = Fam::N, LD = warp_ld(N);
     using A = Arith<F>;
+    using JS = typename Fam::JState;
     const Fam& fam;
     const GsbMethod& m;
     const GsbOptions& o;
@@ -296,23 +431,22 @@ template <class Fam, int T, bool F, bool Mixed, bool PlainRef> struct WarpSolver
     __device__ __forceinline__ double Fr(double xl) const { return fam.template F<T>(tm, tm.lane, xl); }
 
     // J v with the held Jacobian, row `lane`, as a left fold over the columns.
-    __device__ __forceinline__ double jmul(double diag_i, double vl) const {
+    __device__ __forceinline__ double jmul(const JS& js, double vl) const {
         const int i = tm.lane < N ? tm.lane : N - 1;
-        double s = A::mul(fam.J(i, 0, diag_i), tm.bcast(vl, 0));
-        for (int k = 1; k < N; ++k) s = A::madd(fam.J(i, k, diag_i), tm.bcast(vl, k), s);
+        double s = A::mul(fam.Jent(js, i, 0), tm.bcast(vl, 0));
+        for (int k = 1; k < N; ++k) s = A::madd(fam.Jent(js, i, k), tm.bcast(vl, k), s);
         return s;
     }
 
     // grad_ratio_and_norm, src/nonlinear/newton.jl:1287-1298.
-    __device__ void grad_ratio_and_norm(double diag_i, double Fl, double fnorm, double& gr,
+    __device__ void grad_ratio_and_norm(const JS& js, double Fl, double fnorm, double& gr,
                                         double& jnorm) const {
-        // ‖J‖_F as the column-major left fold: every lane folds all entries (the diagonal
-        // arrives by broadcast, the rest is A)
+        // ‖J‖_F as the column-major left fold: every lane folds all entries
         double s = 0.0;
         for (int k = 0; k < N; ++k) {
-            const double dk = tm.bcast(diag_i, k);
+            const double dk = fam.template col_diag<T>(tm, js, k);
             for (int i = 0; i < N; ++i) {
-                const double v = i == k ? dk : fam.A(i, k);
+                const double v = fam.Jall(js, i, k, dk);
                 s = (i == 0 && k == 0) ? A::mul(v, v) : A::madd(v, v, s);
             }
         }
@@ -321,9 +455,8 @@ template <class Fam, int T, bool F, bool Mixed, bool PlainRef> struct WarpSolver
         if (!direct) {
             // the scaled fallback of rnorm over the N*N entries
             for (int k = 0; k < N; ++k) {
-                const double dk = tm.bcast(diag_i, k);
-                for (int i = 0; i < N; ++i)
-                    mx = jmax(mx, jmax(fabs(i == k ? dk : fam.A(i, k)), 0.0));
+                const double dk = fam.template col_diag<T>(tm, js, k);
+                for (int i = 0; i < N; ++i) mx = jmax(mx, jmax(fabs(fam.Jall(js, i, k, dk)), 0.0));
             }
         }
         if (direct) {
@@ -334,9 +467,9 @@ template <class Fam, int T, bool F, bool Mixed, bool PlainRef> struct WarpSolver
             const int e = jexponent(mx);
             double acc = 0.0;
             for (int k = 0; k < N; ++k) {
-                const double dk = tm.bcast(diag_i, k);
+                const double dk = fam.template col_diag<T>(tm, js, k);
                 for (int i = 0; i < N; ++i) {
-                    const double u = scale2_in(i == k ? dk : fam.A(i, k), -e);
+                    const double u = scale2_in(fam.Jall(js, i, k, dk), -e);
                     acc = (i == 0 && k == 0) ? A::mul(u, u) : A::madd(u, u, acc);
                 }
             }
@@ -346,11 +479,10 @@ template <class Fam, int T, bool F, bool Mixed, bool PlainRef> struct WarpSolver
             gr = 0.0;
             return;
         }
-        // g_j = sum_i J_ij F_i: lane j folds column j
+        // g_j = sum_i J_ij F_i: lane j folds column j (its own diagonal entry where i == j)
         const int j = tm.lane < N ? tm.lane : N - 1;
-        const double dj = diag_i;
-        double g = A::mul(fam.J(0, j, tm.bcast(dj, 0)), tm.bcast(Fl, 0));
-        for (int i = 1; i < N; ++i) g = A::madd(i == j ? dj : fam.A(i, j), tm.bcast(Fl, i), g);
+        double g = A::mul(fam.Jent(js, 0, j), tm.bcast(Fl, 0));
+        for (int i = 1; i < N; ++i) g = A::madd(fam.Jent(js, i, j), tm.bcast(Fl, i), g);
         const double gnorm = wv.rnorm(g);
         if (isfin(gnorm) || !(isfin(jnorm) && isfin(fnorm))) {
             gr = __ddiv_rn(__ddiv_rn(gnorm, jnorm), fnorm);
@@ -358,9 +490,8 @@ template <class Fam, int T, bool F, bool Mixed, bool PlainRef> struct WarpSolver
         }
         const int e = jexponent(fnorm);
         const double sc = ldexp(1.0, -e);
-        g = A::mul(fam.J(0, j, tm.bcast(dj, 0)), __dmul_rn(tm.bcast(Fl, 0), sc));
-        for (int i = 1; i < N; ++i)
-            g = A::madd(i == j ? dj : fam.A(i, j), __dmul_rn(tm.bcast(Fl, i), sc), g);
+        g = A::mul(fam.Jent(js, 0, j), __dmul_rn(tm.bcast(Fl, 0), sc));
+        for (int i = 1; i < N; ++i) g = A::madd(fam.Jent(js, i, j), __dmul_rn(tm.bcast(Fl, i), sc), g);
         gr = __ddiv_rn(__ddiv_rn(wv.rnorm(g), jnorm), ldexp(fnorm, -e));
     }
 
@@ -501,12 +632,12 @@ template <class Fam, int T, bool F, bool Mixed, bool PlainRef> struct WarpSolver
 
     // refine_passes!! with the held Jacobian (refinement.jl:211-244); returns `failed`.
     template <class Fac>
-    __device__ bool refine(double& dl, const Fac& fac, double diag_i, double Fl) const {
+    __device__ bool refine(double& dl, const Fac& fac, const JS& js, double Fl) const {
         const double fnorm = wv.rnorm(Fl);
         if (fnorm == 0.0) return false;
         if (!isfin(fnorm)) return true;
         const double thr = __dmul_rn(jmax(m.refine_eta, kSqrtEps), fnorm);
-        double r = jmul(diag_i, dl);
+        double r = jmul(js, dl);
         r = __dadd_rn(-Fl, -r);
         double rprev = wv.rnorm(r);
         if (!isfin(rprev)) return true;
@@ -514,7 +645,7 @@ template <class Fam, int T, bool F, bool Mixed, bool PlainRef> struct WarpSolver
         for (int it = 1; it <= m.refine_maxiter; ++it) {
             double dc = fac.ldiv(tm, wv, r);
             dc = __dadd_rn(dl, dc);
-            r = jmul(diag_i, dc);
+            r = jmul(js, dc);
             r = __dadd_rn(-Fl, -r);
             const double rc = wv.rnorm(r);
             if (!(rc < rprev)) return true;
@@ -527,17 +658,17 @@ template <class Fam, int T, bool F, bool Mixed, bool PlainRef> struct WarpSolver
 
     __device__ void step_plain(DevState& st, double& xl, double& Fl, StepInfo& info) const {
         const double fnorm = residual_norm(st, Fl);
-        const double diag_i = fam.diag(tm.lane, xl);
+        const JS js = fam.template jacobian<T>(tm, xl);
         double gr, jn;
-        grad_ratio_and_norm(diag_i, Fl, fnorm, gr, jn);
+        grad_ratio_and_norm(js, Fl, fnorm, gr, jn);
         double merit = st.merit;
         WarpLU<N, T, F, double> fac{lu};
-        fac.factor(tm, fam, diag_i);
+        fac.factor(tm, fam, js);
         if (fac.info > 0) {
             info = {SINGULAR, wv.rnorm(Fl), 0.0, 0, false, false, false};
         } else {
             double dl = -fac.ldiv(tm, wv, Fl);
-            if constexpr (PlainRef) refine(dl, fac, diag_i, Fl);
+            if constexpr (PlainRef) refine(dl, fac, js, Fl);
             globalize(xl, Fl, dl, !PlainRef, merit, info);
         }
         st.gradratio = gr;
@@ -549,9 +680,9 @@ template <class Fam, int T, bool F, bool Mixed, bool PlainRef> struct WarpSolver
     __device__ void step_mixed(DevState& st, double& xl, double& Fl, StepInfo& info) const {
         const double fnorm_old = residual_norm(st, Fl);
         const bool was_promoted = st.promoted;
-        const double diag_i = fam.diag(tm.lane, xl);
+        const JS js = fam.template jacobian<T>(tm, xl);
         double gr, jn;
-        grad_ratio_and_norm(diag_i, Fl, fnorm_old, gr, jn);
+        grad_ratio_and_norm(js, Fl, fnorm_old, gr, jn);
         st.gradratio = gr;
         st.jnorm = jn;
         const bool ref = m.refinement == GSB_REFINEMENT;
@@ -563,13 +694,13 @@ template <class Fam, int T, bool F, bool Mixed, bool PlainRef> struct WarpSolver
         bool fallback = was_promoted;
         if (!was_promoted) {
             WarpLU<N, T, F, float> fac{reinterpret_cast<float*>(lu)};
-            fac.factor(tm, fam, diag_i);
+            fac.factor(tm, fam, js);
             bool ref_failed;
             if (fac.info > 0) {
                 ref_failed = true;
             } else {
                 dl = -fac.ldiv(tm, wv, Fl);
-                ref_failed = ref ? refine(dl, fac, diag_i, Fl) : false;
+                ref_failed = ref ? refine(dl, fac, js, Fl) : false;
             }
             if (ref_failed || fac.info > 0) {
                 failures += 1;
@@ -578,18 +709,18 @@ template <class Fam, int T, bool F, bool Mixed, bool PlainRef> struct WarpSolver
             } else if (fnorm_old == 0.0 || !isfin(fnorm_old)) {
                 lin_rel = 0.0;
             } else {
-                const double lin = __dadd_rn(Fl, jmul(diag_i, dl));
+                const double lin = __dadd_rn(Fl, jmul(js, dl));
                 lin_rel = __ddiv_rn(wv.rnorm(lin), fnorm_old);
             }
         }
         if (fallback) {
             WarpLU<N, T, F, double> ft{lu};
-            ft.factor(tm, fam, diag_i);
+            ft.factor(tm, fam, js);
             if (ft.info > 0) {
                 ok = false;
             } else {
                 dl = -ft.ldiv(tm, wv, Fl);
-                if (was_promoted && ref) refine(dl, ft, diag_i, Fl);
+                if (was_promoted && ref) refine(dl, ft, js, Fl);
             }
         }
         if (!ok) {

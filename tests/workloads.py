@@ -98,3 +98,27 @@ def c4(nsys=4194304):
         idx = p_off[sel][:, None] + np.arange(n * n + n)[None, :]
         P[idx] = Pb
     return sizes, np.zeros(int(n64.sum()), dtype=np.float64), P
+
+
+def henon_heiles_energy(s):
+    q1, q2, p1, p2 = s[:, 0], s[:, 1], s[:, 2], s[:, 3]
+    return 0.5 * (p1 * p1 + p2 * p2) + 0.5 * (q1 * q1 + q2 * q2) + q1 * q1 * q2 - q2 ** 3 / 3.0
+
+
+def c3_states(nsys, config_id=3, stream=0, box=0.6):
+    """Hénon–Heiles states (q1, q2, p1, p2) uniform in [-box, box]^4, rejection-sampled to energy
+    H in [0.01, 0.16]. The training set of the warm start draws from its own stream."""
+    g = rng(config_id, stream)
+    out = np.empty((0, 4))
+    while out.shape[0] < nsys:
+        s = g.uniform(-box, box, (2 * (nsys - out.shape[0]) + 1024, 4))
+        H = henon_heiles_energy(s)
+        out = np.concatenate([out, s[(H >= 0.01) & (H <= 0.16)]])
+    return np.ascontiguousarray(out[:nsys])
+
+
+def c3(nsys=262144):
+    """The Gauss-3 stage systems of one h = 0.1 step from each state: Z0 = 0 (12 unknowns) and
+    P = the state (4 per system)."""
+    P = c3_states(nsys)
+    return np.zeros((nsys, 12)), P

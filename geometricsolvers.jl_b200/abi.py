@@ -174,6 +174,7 @@ EXPORTED_SYMBOLS = (
     "gsb_solve_batch_counts_noalloc",
     "gsb_uneven_sizes",
     "gsb_solve_batch_uneven",
+    "gsb_umma_selftest",
 )
 
 _lib = None
@@ -225,5 +226,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
     ]
     lib.gsb_solve_batch_uneven.restype = ctypes.c_int
+    lib.gsb_umma_selftest.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                      ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p]
+    lib.gsb_umma_selftest.restype = ctypes.c_int
     _lib = lib
     return lib

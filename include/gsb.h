@@ -297,6 +297,15 @@ GSB_API int gsb_solve_batch_uneven(const GsbMethod* method, const GsbOptions* op
                                    const int64_t* x_off, const int64_t* p_off, int64_t nsys,
                                    const GsbBucketConfig* table, void* stream, GsbTally* tally);
 
+/* ─── the learned warm start of the stage systems (no counterpart in the reference) ────────── */
+
+/* Self-test of the tensor-core tile product the warm-start network is built on: D (128 x N,
+ * FP32, row-major) = A B^T for BF16 operands, A 128 x K and B N x K row-major (mode 0), or A
+ * given as its K x 128 transpose and B as its K x N transpose (mode 1). 16 <= K <= 128 and
+ * 16 <= N <= 256, multiples of 16. Device pointers; returns after the product is written. */
+GSB_API int gsb_umma_selftest(const uint16_t* A, const uint16_t* B, float* D, int32_t K, int32_t N,
+                              int32_t mode, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

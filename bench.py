@@ -44,9 +44,10 @@ def parse():
     ap.add_argument("--profile", choices=["plain", "mixed", "lm"], default=None,
                     help="run `--warmup` + `--steps` solves of one form only (for ncu captures): "
                          "the cubic-affine batch of size --n, or the exponential-sum fit (lm)")
-    ap.add_argument("--workload", choices=["c1", "c0", "c2", "c4"], default="c1",
+    ap.add_argument("--workload", choices=["c1", "c0", "c2", "c3", "c4"], default="c1",
                     help="c1 (default): the n = 8 batch of the headline metric; c0: n = 3, "
-                         "65,536 systems; c2: the exponential-sum least-squares fit; c4: the "
+                         "65,536 systems; c2: the exponential-sum least-squares fit; c3: the "
+                         "Gauss-3 stage systems with the learned warm start; c4: the "
                          "ragged batch of sizes 2..32 (one GPU)")
     ap.add_argument("--n", type=int, default=N_UNKNOWNS,
                     help="cubic-affine size of a --profile run (A = 6I + ... at n = 8, else (n+1)I)")
@@ -564,6 +565,121 @@ def _roof(bytes_total, flops, kms, peaks, hbm_peak, hbm_src, kernel):
     return r
 
 
+def run_c3(args, opts, hbm_peak, hbm_src, peaks):
+    """The stage systems: plain Newton from Z = 0 against the learned warm start (the network
+    trained first, on 2,097,152 plain-solver solutions of a disjoint draw; its training time is
+    reported, not timed in the step)."""
+    import torch
+
+    import gsb200 as G
+    from oracle import oracle_py as O
+    from workloads import c3, c3_states
+
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.current_stream(dev)
+    nsys = args.nsys if args.nsys != NSYS else 262144
+    fam = G.IrkHenonHeiles(0.1)
+    prob = G.NonlinearProblem(fam)
+    plain = G.Newton(globalization=G.Backtracking())
+    ntr = 2097152
+    tr = c3_states(ntr, stream=1)
+    Ztr = torch.zeros(ntr, 12, dtype=torch.float64, device=dev)
+    G.solve_batch(Ztr, G.status_buffer(ntr), prob, plain,
+                  G.PerSystem(torch.tensor(tr, device=dev)), options=opts)
+    net = G.MlpWarmStart(fam, seed=0)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    hist = net.train(tr, Ztr.cpu().numpy(), epochs=80, batch=8192, lr=5e-3)
+    torch.cuda.synchronize()
+    t_train = time.perf_counter() - t0
+    X0_h, P_h = c3(nsys)
+    X0 = torch.tensor(X0_h, device=dev)
+    P = torch.tensor(P_h, device=dev)
+    ps = G.PerSystem(P)
+    X = torch.empty_like(X0)
+    S = G.status_buffer(nsys)
+
+    def step_plain():
+        X.copy_(X0)
+        G.solve_batch(X, S, prob, plain, ps, options=opts)
+
+    Xw = torch.empty_like(X0)
+    acc_last = {}
+
+    def step_warm():
+        Z, acc = net.warm_start(P, X0)
+        Xw.copy_(Z)
+        G.solve_batch(Xw, S, prob, plain, ps, options=opts)
+        acc_last["acc"] = acc
+
+    xo, so = O.solve_batch(prob, plain, X0_h.copy(), P_h, opts)
+    forms = {}
+    with Clocks(0) as clk:
+        for name, step, xbuf in (("plain_fp64", step_plain, X), ("mlp_warm_start", step_warm, Xw)):
+            ms = _events_ms(step, args.steps, args.warmup, stream)
+            step()
+            st = G.statuses(S)
+            err = rel_err(xbuf.cpu().numpy(), xo)
+            ok = (st["code"] == so["code"]) & (err <= REL_TOL)
+            forms[name] = {"systems_per_s": float(np.sum(ok)) / (ms * 1e-3), "ms_per_step": ms,
+                           "solved": int(np.sum(ok)), "mean_iterations": float(st["iterations"].mean()),
+                           "fp64_oracle_max_rel_err": float(err.max())}
+    clocks = clk.summary()
+    forms["mlp_warm_start"]["fallback_rate"] = 1.0 - float(acc_last["acc"].float().mean().item())
+    forms["mlp_warm_start"]["training"] = {"samples": ntr, "epochs": 80, "batch": 8192,
+                                           "seconds": t_train, "loss_first": hist[0],
+                                           "loss_last": hist[-1]}
+    chosen = max(("plain_fp64", "mlp_warm_start"), key=lambda k: forms[k]["systems_per_s"])
+    forms["chosen_over_plain"] = forms[chosen]["systems_per_s"] / forms["plain_fp64"]["systems_per_s"]
+    value = forms[chosen]["systems_per_s"]
+    ms = forms[chosen]["ms_per_step"]
+    kms = forms["plain_fp64"]["ms_per_step"] - _events_ms(lambda: X.copy_(X0), 20, 2, stream)
+    flops = float(np.sum(flops_per_system(12, so["iterations"].astype(np.int64),
+                                          1 + _trials(so))))
+    bytes_total = (32 + 96 + 96 + 72) * nsys
+    x_pin = torch.from_numpy(X0_h).pin_memory()
+    p_pin = torch.from_numpy(P_h).pin_memory()
+    x_out = torch.empty_like(x_pin).pin_memory()
+    s_out = torch.empty((nsys, 72), dtype=torch.uint8).pin_memory()
+    Pe, Xe = torch.empty_like(P), torch.empty_like(X0)
+
+    def e2e():
+        Pe.copy_(p_pin, non_blocking=True)
+        Xe.copy_(x_pin, non_blocking=True)
+        if chosen == "mlp_warm_start":
+            Z, _ = net.warm_start(Pe, Xe)
+            Xe.copy_(Z)
+        G.solve_batch(Xe, S, prob, plain, G.PerSystem(Pe), options=opts)
+        x_out.copy_(Xe, non_blocking=True)
+        s_out.copy_(S, non_blocking=True)
+
+    ms_e2e = _events_ms(e2e, max(1, args.steps // 2), 1, stream)
+    sample = min(nsys, 65536)
+    cpu = _cpu_sample(lambda nt: O.solve_batch(prob, plain, X0_h[:sample].copy(), P_h[:sample],
+                                               opts, nthreads=nt), sample, "c3, plain from Z = 0")
+    line = {
+        "metric": METRIC, "value": value, "unit": "systems/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded; the configuration's shapes and distributions)",
+        "config": {"workload": f"Gauss-3 stage systems of the Hénon–Heiles field, h = 0.1, n = 12, "
+                               f"{nsys} systems, Newton + LU + Backtracking; learned warm start "
+                               "(4-128-128-12 MLP, BF16 tcgen05) with the accept-if-better gate",
+                   "chosen_form": chosen, "global_batch": nsys, "parallelism": "one GPU",
+                   "l2": "inputs fit in L2; a step rewrites X from X0"},
+        "forms": forms,
+        "e2e": {"value": value * ms / ms_e2e, "unit": "systems/s",
+                "h2d_bytes_per_step": int(X0_h.nbytes + P_h.nbytes),
+                "d2h_bytes_per_step": int(X0_h.nbytes + nsys * 72), "ms_per_step": ms_e2e},
+        "gpu_launches": args.steps * (3 if chosen == "mlp_warm_start" else 1),
+        "roofline": _roof(bytes_total, flops, kms, peaks, hbm_peak, hbm_src,
+                          "warp_kernel<WarpIrk, 16, fused, FP64>"),
+        "cpu_baseline": cpu,
+        "clocks": clocks,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def run_workload(args):
     import torch
 
@@ -578,6 +694,8 @@ def run_workload(args):
     peaks = fp_peaks()
     forms = {}
 
+    if args.workload == "c3":
+        return run_c3(args, opts, hbm_peak, hbm_src, peaks)
     if args.workload in ("c0", "c2"):
         if args.workload == "c0":
             from workloads import c0

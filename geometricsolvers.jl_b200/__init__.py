@@ -36,6 +36,7 @@ from .api import (
     statuses,
 )
 from .batch import batch_summary, ragged_offsets, solve_batch, solve_batch_uneven
-from . import tune
+from . import tune, warmstart
+from .warmstart import MlpWarmStart
 
 __all__ = [name for name in dir() if not name.startswith("_")]

@@ -175,6 +175,12 @@ EXPORTED_SYMBOLS = (
     "gsb_uneven_sizes",
     "gsb_solve_batch_uneven",
     "gsb_umma_selftest",
+    "gsb_mlp_sizes",
+    "gsb_mlp_pack",
+    "gsb_mlp_predict",
+    "gsb_mlp_grad",
+    "gsb_mlp_adam",
+    "gsb_warm_start_select",
 )
 
 _lib = None
@@ -229,5 +235,16 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.gsb_umma_selftest.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                       ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p]
     lib.gsb_umma_selftest.restype = ctypes.c_int
+    V = ctypes.c_void_p
+    lib.gsb_mlp_sizes.argtypes = [ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)]
+    lib.gsb_mlp_pack.argtypes = [V, V, V]
+    lib.gsb_mlp_predict.argtypes = [V, V, V, V, V, V, ctypes.c_int64, V, V]
+    lib.gsb_mlp_grad.argtypes = [V, V, V, V, V, ctypes.c_int64, V, V, V, V]
+    lib.gsb_mlp_adam.argtypes = [V, V, V, V, V, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                                 ctypes.c_float, ctypes.c_int32, V]
+    lib.gsb_warm_start_select.argtypes = [V, V, V, V, V, V, ctypes.c_int64, V]
+    for f in ("gsb_mlp_sizes", "gsb_mlp_pack", "gsb_mlp_predict", "gsb_mlp_grad", "gsb_mlp_adam",
+              "gsb_warm_start_select"):
+        getattr(lib, f).restype = ctypes.c_int
     _lib = lib
     return lib

@@ -306,6 +306,36 @@ GSB_API int gsb_solve_batch_uneven(const GsbMethod* method, const GsbOptions* op
 GSB_API int gsb_umma_selftest(const uint16_t* A, const uint16_t* B, float* D, int32_t K, int32_t N,
                               int32_t mode, void* stream);
 
+/* The network: a 4 -> 128 -> 128 -> 12 MLP (GELU, BF16 weights and activations in the
+ * tensor-core products, FP32 accumulation) giving the start Z0 = g(y) + scale * net((y - mean)
+ * * inv_dev) of the Gauss-3 stage equations of a Hénon–Heiles state y, where g(y)_j = h c_j f(y)
+ * is the explicit stage guess. theta holds gsb_mlp_sizes' theta_floats FP32 parameters: W1
+ * [128][4], b1 [128], W2 [128][128] (in, out), b2 [128], W3 [128][16] (in, out; outputs 12..15
+ * zero), b3 [16]; pack holds its BF16 copies (pack_halves), written by gsb_mlp_pack and
+ * gsb_mlp_adam; norm holds mean (4), inv_dev (4), scale (12). `shared` is the stage family's
+ * (h, A column-major). err_scratch is one device int. All pointers are device pointers. */
+GSB_API int gsb_mlp_sizes(int64_t* theta_floats, int64_t* pack_halves);
+GSB_API int gsb_mlp_pack(const float* theta, uint16_t* pack, void* stream);
+/* Z0 (n x 12) for the states (n x 4); returns after Z0 is written. */
+GSB_API int gsb_mlp_predict(const float* theta, const uint16_t* pack, const float* norm,
+                            const double* shared, const double* states, double* Z0, int64_t n,
+                            int* err_scratch, void* stream);
+/* The gradient of the mean squared error of the network's output against `targets` (n x 12,
+ * the scaled corrections (Z - g(y)) / scale) into grad (theta_floats), and the sum of squared
+ * errors into loss; stream-ordered. */
+GSB_API int gsb_mlp_grad(const float* theta, const uint16_t* pack, const float* norm,
+                         const double* states, const float* targets, int64_t n, float* grad,
+                         float* loss, int* err_scratch, void* stream);
+/* One bias-corrected Adam step (step >= 1) on theta with moments m, v; refreshes pack. */
+GSB_API int gsb_mlp_adam(float* theta, float* m, float* v, const float* grad, uint16_t* pack,
+                         float lr, float beta1, float beta2, float eps, int32_t step, void* stream);
+/* The accept-if-better gate: per system, X = the start (Z0 or Xdefault, n x 12) whose FP64
+ * residual norm of the stage equations is smaller (Xdefault on ties and non-finite Z0), and
+ * accepted = 1 where Z0 was taken. */
+GSB_API int gsb_warm_start_select(const double* shared, const double* states, const double* Z0,
+                                  const double* Xdefault, double* X, uint8_t* accepted, int64_t n,
+                                  void* stream);
+
 #ifdef __cplusplus
 }
 #endif

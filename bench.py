@@ -41,7 +41,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="gsb200", choices=["gsb200", "reference"])
     ap.add_argument("--nsys", type=int, default=NSYS)
-    ap.add_argument("--profile", choices=["plain", "mixed", "lm"], default=None,
+    ap.add_argument("--profile", choices=["plain", "mixed", "lm", "irk", "mlp"], default=None,
                     help="run `--warmup` + `--steps` solves of one form only (for ncu captures): "
                          "the cubic-affine batch of size --n, or the exponential-sum fit (lm)")
     ap.add_argument("--workload", choices=["c1", "c0", "c2", "c3", "c4"], default="c1",
@@ -475,7 +475,27 @@ def run_profile(args):
 
     import gsb200 as G
 
-    if args.profile == "lm":
+    if args.profile == "mlp":
+        # gradient steps of the warm-start network on args.nsys states (random targets)
+        from workloads import c3_states
+
+        net = G.MlpWarmStart(G.IrkHenonHeiles(0.1), seed=0)
+        st_h = c3_states(args.nsys, stream=1)
+        net.set_normalisation(st_h, net.stage_guess(st_h))
+        S_ = torch.tensor(st_h, device="cuda")
+        T_ = torch.randn(args.nsys, 12, dtype=torch.float32, device="cuda")
+        for _ in range(args.warmup + args.steps):
+            net.gradient(S_, T_)
+        torch.cuda.synchronize()
+        print(json.dumps({"profile": "mlp", "nsys": args.nsys, "err": int(net.err.item())}))
+        return
+    if args.profile == "irk":
+        from workloads import c3
+
+        X0_h, P_h = c3(args.nsys)
+        prob = G.NonlinearProblem(G.IrkHenonHeiles(0.1))
+        m = G.Newton(globalization=G.Backtracking())
+    elif args.profile == "lm":
         from workloads import c2
 
         X0_h, P_h, t = c2(args.nsys)

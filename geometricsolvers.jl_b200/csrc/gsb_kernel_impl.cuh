@@ -54,12 +54,13 @@ __device__ __forceinline__ Range launch_range(const Launch& L) {
     return {L.nsys, L.order};
 }
 
-// The CTA's chunks: one per CTA, or, with a work queue, chunks taken from the counter until the
-// batch is exhausted (systems_per_chunk systems each).
-template <class Body>
+// The CTA's chunks: one per CTA, or (persistent launches) chunks taken from the work queue
+// until the batch is exhausted (systems_per_chunk systems each).
+template <bool Persistent, class Body>
 __device__ __forceinline__ void for_each_chunk(const Launch& L, int64_t systems_per_chunk, Body body) {
     const Range r = launch_range(L);
-    if (L.queue == nullptr) {
+    if constexpr (!Persistent) {
+        // one chunk per CTA: no loop around the solve, whose registers it would hold
         body((int64_t)blockIdx.x * systems_per_chunk, r);
         return;
     }
@@ -167,13 +168,15 @@ template <class Fam, bool Mixed> constexpr int min_blocks() {
 #endif
 }
 
-template <class Fam, bool F, bool Mixed, bool PlainRef>
-__global__ void __launch_bounds__(kThreads, (min_blocks<Fam, Mixed>())) newton_kernel(GsbMethod m, GsbOptions o, Launch L) {
+template <class Fam, bool F, bool Mixed, bool PlainRef, bool Persistent>
+__global__ void __launch_bounds__(kThreads, (min_blocks<Fam, Mixed>())) newton_kernel(const __grid_constant__ GsbMethod m,
+                                 const __grid_constant__ GsbOptions o,
+                                 const __grid_constant__ Launch L) {
     extern __shared__ double smem[];
     constexpr int N = Fam::N, NP = Fam::NP, RS = row_stride(NP, N);
     const int tid = threadIdx.x;
     double* prow = smem + tid * RS;
-    for_each_chunk(L, kThreads, [&](int64_t base, const Range& r) {
+    for_each_chunk<Persistent>(L, kThreads, [&](int64_t base, const Range& r) {
         const int64_t i = base + tid;
         if (r.order == nullptr && L.p_layout == GSB_AOS && L.p_off == nullptr) {
             stage_aos<NP, RS, kThreads>(smem, L.P + base * NP, r.n - base, tid);
@@ -214,14 +217,16 @@ __global__ void __launch_bounds__(kThreads, (min_blocks<Fam, Mixed>())) newton_k
 
 // The team form: T lanes per system, kThreads / T systems per CTA, each system's parameter block
 // staged into a shared-memory row that its lanes read.
-template <class Fam, int T, bool Mixed>
-__global__ void __launch_bounds__(kThreads) team_kernel(GsbMethod m, GsbOptions o, Launch L) {
+template <class Fam, int T, bool Mixed, bool Persistent>
+__global__ void __launch_bounds__(kThreads) team_kernel(const __grid_constant__ GsbMethod m,
+                                 const __grid_constant__ GsbOptions o,
+                                 const __grid_constant__ Launch L) {
     extern __shared__ double smem[];
     constexpr int N = Fam::N, NP = Fam::NP, RS = (NP % 2 == 1) ? NP : NP + 1;
     constexpr int SPB = kThreads / T;
     const int tid = threadIdx.x;
     const int team = tid / T;
-    for_each_chunk(L, SPB, [&](int64_t base, const Range& r) {
+    for_each_chunk<Persistent>(L, SPB, [&](int64_t base, const Range& r) {
         const int64_t i = base + team;
         if (r.order == nullptr && L.p_layout == GSB_AOS && L.p_off == nullptr) {
             stage_aos<NP, RS, SPB>(smem, L.P + base * NP, r.n - base, tid);
@@ -262,7 +267,9 @@ __global__ void __launch_bounds__(kThreads) team_kernel(GsbMethod m, GsbOptions 
 // The least-squares form: one Levenberg–Marquardt solve per thread. Shared memory holds each
 // system's M observations (odd row stride) and, after the rows, the M abscissae of the batch.
 template <class Fam, bool F>
-__global__ void __launch_bounds__(kThreads, 3) lm_kernel(GsbMethod m, GsbOptions o, Launch L) {
+__global__ void __launch_bounds__(kThreads, 3) lm_kernel(const __grid_constant__ GsbMethod m,
+                                 const __grid_constant__ GsbOptions o,
+                                 const __grid_constant__ Launch L) {
     extern __shared__ double smem[];
     constexpr int N = Fam::N, M = Fam::M, RS = (M % 2 == 1) ? M : M + 1;
     const int tid = threadIdx.x;
@@ -316,14 +323,16 @@ template <class Fam> struct WarpPlace {
     __device__ __forceinline__ int operator()(int k) const { return Fam::place(k); }
 };
 
-template <class Fam, int T, bool F, bool Mixed, bool PlainRef>
-__global__ void __launch_bounds__(kThreads) warp_kernel(GsbMethod m, GsbOptions o, Launch L) {
+template <class Fam, int T, bool F, bool Mixed, bool PlainRef, bool Persistent>
+__global__ void __launch_bounds__(kThreads) warp_kernel(const __grid_constant__ GsbMethod m,
+                                 const __grid_constant__ GsbOptions o,
+                                 const __grid_constant__ Launch L) {
     extern __shared__ double smem[];
     constexpr int N = Fam::N, NP = Fam::NP, SPB = kThreads / T, SS = warp_sys_stride<Fam>();
     const int tid = threadIdx.x;
     const int team = tid / T;
     double* sys = smem + team * SS;
-    for_each_chunk(L, SPB, [&](int64_t base, const Range& r) {
+    for_each_chunk<Persistent>(L, SPB, [&](int64_t base, const Range& r) {
         const int64_t i = base + team;
         if (r.order == nullptr && L.p_layout == GSB_AOS && L.p_off == nullptr) {
             stage_aos<NP, SS, SPB>(smem, L.P + base * NP, r.n - base, tid, WarpPlace<Fam>());
@@ -361,26 +370,29 @@ __global__ void __launch_bounds__(kThreads) warp_kernel(GsbMethod m, GsbOptions 
 using KernelFn = void (*)(GsbMethod, GsbOptions, Launch);
 
 struct KernelEntry {
-    KernelFn fn;
+    KernelFn fn;             // one chunk per CTA
+    KernelFn fn_persistent;  // chunks from the launch's work queue
     int smem_doubles;  // dynamic shared memory of a CTA, in doubles
     int systems_per_block;
     bool attr_set[64];
 };
 
 template <class Fam, bool F, bool Mixed, bool PlainRef> KernelEntry* entry() {
-    static KernelEntry e{newton_kernel<Fam, F, Mixed, PlainRef>,
+    static KernelEntry e{newton_kernel<Fam, F, Mixed, PlainRef, false>,
+                         newton_kernel<Fam, F, Mixed, PlainRef, true>,
                          kThreads * row_stride(Fam::NP, Fam::N), kThreads, {}};
     return &e;
 }
 
 template <class Fam, bool F> KernelEntry* lm_entry() {
     constexpr int RS = (Fam::M % 2 == 1) ? Fam::M : Fam::M + 1;
-    static KernelEntry e{lm_kernel<Fam, F>, kThreads * RS + Fam::M, kThreads, {}};
+    static KernelEntry e{lm_kernel<Fam, F>, nullptr, kThreads * RS + Fam::M, kThreads, {}};
     return &e;
 }
 
 template <class Fam, int T, bool F, bool Mixed, bool PlainRef> KernelEntry* warp_entry() {
-    static KernelEntry e{warp_kernel<Fam, T, F, Mixed, PlainRef>,
+    static KernelEntry e{warp_kernel<Fam, T, F, Mixed, PlainRef, false>,
+                         warp_kernel<Fam, T, F, Mixed, PlainRef, true>,
                          (kThreads / T) * warp_sys_stride<Fam>(), kThreads / T, {}};
     return &e;
 }
@@ -397,7 +409,8 @@ template <class Fam, int T> KernelEntry* pick_warp(bool fused, bool mixed, bool 
 
 template <class Fam, int T, bool Mixed> KernelEntry* team_entry() {
     constexpr int RS = (Fam::NP % 2 == 1) ? Fam::NP : Fam::NP + 1;
-    static KernelEntry e{team_kernel<Fam, T, Mixed>, (kThreads / T) * RS, kThreads / T, {}};
+    static KernelEntry e{team_kernel<Fam, T, Mixed, false>, team_kernel<Fam, T, Mixed, true>,
+                         (kThreads / T) * RS, kThreads / T, {}};
     return &e;
 }
 

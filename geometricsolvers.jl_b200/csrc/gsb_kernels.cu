@@ -775,16 +775,17 @@ int uneven_entry(const UnevenKey& k, int b, int sms, KernelEntry** ke, unsigned*
     const size_t smem = (size_t)(*ke)->smem_doubles * sizeof(double);
     int dev = 0;
     if (int rc = cuda_err(cudaGetDevice(&dev), "cudaGetDevice")) return rc;
-    if (!(*ke)->attr_set[dev & 63]) {
-        if (int rc = cuda_err(cudaFuncSetAttribute(reinterpret_cast<const void*>((*ke)->fn),
-                                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                   (int)smem), "cudaFuncSetAttribute"))
-            return rc;
-        (*ke)->attr_set[dev & 63] = true;
-    }
+    (void)dev;
+    if (!(*ke)->fn_persistent) return set_err(GSB_ERR_UNSUPPORTED, "no persistent bucket kernel");
+    // the persistent form of the bucket's kernel (set once per capture, which is rare)
+    if (int rc = cuda_err(cudaFuncSetAttribute(reinterpret_cast<const void*>((*ke)->fn_persistent),
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               (int)smem), "cudaFuncSetAttribute"))
+        return rc;
     int occ = 0;
     if (int rc = cuda_err(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                              &occ, reinterpret_cast<const void*>((*ke)->fn), kThreads, smem),
+                              &occ, reinterpret_cast<const void*>((*ke)->fn_persistent), kThreads,
+                              smem),
                           "occupancy"))
         return rc;
     if (occ < 1) return set_err(GSB_ERR_UNSUPPORTED, "a bucket kernel does not fit on an SM");
@@ -821,7 +822,7 @@ int uneven_capture(UnevenPlan& p, const UnevenKey& k, bool want_tally) {
         Launch L{k.X, GSB_AOS, k.S, k.s_kind, k.P, GSB_AOS, p.list, 0, k.nsys, nullptr,
                  want_tally ? p.work->tally : nullptr, k.x_off, k.p_off, &p.work->queue[b],
                  &p.work->range[b][0]};
-        ke[b]->fn<<<grid[b], kThreads, (size_t)ke[b]->smem_doubles * sizeof(double), p.side[b]>>>(
+        ke[b]->fn_persistent<<<grid[b], kThreads, (size_t)ke[b]->smem_doubles * sizeof(double), p.side[b]>>>(
             k.m, k.o, L);
         cudaEventRecord(p.join[b], p.side[b]);
         cudaStreamWaitEvent(p.cs, p.join[b], 0);

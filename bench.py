@@ -359,36 +359,30 @@ def main():
     value = total_solved / (ms_chosen * 1e-3)
     plain_value = sum_over_ranks(solved["plain_fp64"]) / (ms_plain * 1e-3)
 
-    # end to end through the public API: pinned host inputs in, results out, every step
-    x0_pin = torch.from_numpy(X0_h).pin_memory()
+    # end to end through the public API: the batch in pinned host memory, solved by the
+    # pipelined host-buffer call (copies in both directions overlapping the chunk solves); the
+    # call returns when every result is in host memory, so each step is timed by the host clock
+    x_pin = torch.from_numpy(X0_h).pin_memory()
     p_pin = torch.from_numpy(P_h).pin_memory()
-    x_out = torch.empty_like(x0_pin).pin_memory()
+    x_io = torch.empty_like(x_pin).pin_memory()
     s_out = torch.empty((nsys, 72), dtype=torch.uint8).pin_memory()
-    Xe = torch.empty_like(X0)
-    Pe = torch.empty_like(P)
-    pse = G.PerSystem(Pe)
+    pse = G.PerSystem(p_pin)
 
     def e2e_step():
-        Xe.copy_(x0_pin, non_blocking=True)
-        Pe.copy_(p_pin, non_blocking=True)
-        G.solve_batch(Xe, S, prob, chosen_m, pse, options=opts)
-        x_out.copy_(Xe, non_blocking=True)
-        s_out.copy_(S, non_blocking=True)
+        G.solve_batch_host(x_io, s_out, prob, chosen_m, pse, options=opts)
 
-    for _ in range(max(1, args.warmup // 2)):
+    for _ in range(max(1, args.warmup // 4)):
+        x_io.copy_(x_pin)
         e2e_step()
-    torch.cuda.synchronize(dev)
     barrier()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e2e_steps = max(1, args.steps // 2)
-    e0.record(stream)
+    e2e_steps = max(3, args.steps // 10)
+    t_e2e = []
     for _ in range(e2e_steps):
+        x_io.copy_(x_pin)  # the start iterates again (host side, outside the timed call)
+        t0 = time.perf_counter()
         e2e_step()
-    e1.record(stream)
-    torch.cuda.synchronize(dev)
-    barrier()
-    ms_e2e = max_over_ranks(e0.elapsed_time(e1) / e2e_steps)
+        t_e2e.append(time.perf_counter() - t0)
+    ms_e2e = max_over_ranks(statistics.median(t_e2e) * 1e3)
     e2e_value = total_solved / (ms_e2e * 1e-3)
     h2d = X0_h.nbytes + P_h.nbytes
     d2h = X0_h.nbytes + nsys * 72
@@ -457,7 +451,9 @@ def main():
             "chosen_over_plain": value / plain_value,
         },
         "e2e": {"value": e2e_value, "unit": "systems/s", "h2d_bytes_per_step": h2d,
-                "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e},
+                "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e,
+                "api": "gsb_solve_batch_host (pinned host X, P, S; chunks of 131,072 systems)",
+                "timer": "host clock around the blocking call, median of the steps"},
         "gpu_launches": args.steps,
         "roofline": roof,
         "cpu_baseline": cpu,

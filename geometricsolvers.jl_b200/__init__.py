@@ -35,7 +35,8 @@ from .api import (
     status_buffer,
     statuses,
 )
-from .batch import batch_summary, ragged_offsets, solve_batch, solve_batch_uneven
+from .batch import (batch_summary, ragged_offsets, solve_batch, solve_batch_host,
+                    solve_batch_uneven)
 from . import tune, warmstart
 from .warmstart import MlpWarmStart
 

@@ -174,6 +174,7 @@ EXPORTED_SYMBOLS = (
     "gsb_solve_batch_counts_noalloc",
     "gsb_uneven_sizes",
     "gsb_solve_batch_uneven",
+    "gsb_solve_batch_host",
     "gsb_umma_selftest",
     "gsb_mlp_sizes",
     "gsb_mlp_pack",
@@ -232,6 +233,11 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
     ]
     lib.gsb_solve_batch_uneven.restype = ctypes.c_int
+    lib.gsb_solve_batch_host.argtypes = [
+        P(GsbProblem), P(GsbMethod), P(GsbOptions), ctypes.c_void_p, ctypes.c_void_p,
+        ctypes.c_int32, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_void_p,
+    ]
+    lib.gsb_solve_batch_host.restype = ctypes.c_int
     lib.gsb_umma_selftest.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                       ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p]
     lib.gsb_umma_selftest.restype = ctypes.c_int

@@ -3,6 +3,7 @@
 solve_batch(X, S, prob, method, p=None; order, options, **kwargs) -> S      batched.jl:257-287
 solve_batch(X, prob, method, p=None; ...) -> ReturnCodeCounts               batched.jl:289-307
 solve_batch_uneven(X, S, sizes, P, method; ...) -> S   systems of different sizes in one call
+solve_batch_host(X, S, prob, method, p; chunk, ...) -> S   a batch in host memory, pipelined
 Like the reference's `_launch!` (src/nonlinear/batched.jl:183-195) every call waits for its
 kernel before it returns. Host checks raise before any launch, with the reference's messages.
 """
@@ -267,6 +268,61 @@ def solve_batch_uneven(X, S, sizes, P, method, *, x_off=None, p_off=None, table=
             None if tab is None else ctypes.cast(tab, ctypes.c_void_p),
             ctypes.c_void_p(stream.cuda_stream), ctypes.byref(tally))
         _raise_for(rc, lib)
+    if counts_form:
+        return ReturnCodeCounts(*[int(c) for c in tally.counts])
+    return S
+
+
+def solve_batch_host(X, S, prob, method, p, *, chunk=0, options=None, device=None, **kwargs):
+    """Solve a batch whose X ((nsys, n) float64), S ((nsys, 72) uint8 statuses, or None for
+    the count form) and PerSystem parameters live in host memory (pin them with
+    ``tensor.pin_memory()`` for overlapping copies): the batch streams through the device in
+    chunks, the copies in both directions overlapping the solves. Returns S or the counts."""
+    import torch
+
+    if not isinstance(prob, NonlinearProblem):
+        raise ArgumentError("prob must be a NonlinearProblem or a LeastSquaresProblem")
+    fam = prob.family
+    for t, what in ((X, "X"),):
+        if not (isinstance(t, torch.Tensor) and t.device.type == "cpu" and t.dtype == torch.float64
+                and t.is_contiguous()):
+            raise ArgumentError(f"{what} must be a contiguous float64 host tensor")
+    if X.dim() != 2 or X.shape[1] != fam.n:
+        raise DimensionMismatch(f"X must be (nsys, {fam.n}), got {tuple(X.shape)}")
+    nsys = X.shape[0]
+    if not isinstance(p, PerSystem):
+        raise ArgumentError("p must be a PerSystem of per-system parameter blocks")
+    Pt = p.data
+    if not (isinstance(Pt, torch.Tensor) and Pt.device.type == "cpu" and Pt.dtype == torch.float64
+            and Pt.is_contiguous() and Pt.dim() == 2):
+        raise ArgumentError("PerSystem data must be a contiguous (nsys, np) float64 host tensor")
+    if Pt.shape[0] != nsys:
+        raise DimensionMismatch(f"PerSystem parameter length {Pt.shape[0]} does not match batch length {nsys}")
+    if Pt.shape[1] != fam.param_count:
+        raise DimensionMismatch(f"each system takes {fam.param_count} parameters")
+    opt = _resolve_options(options, kwargs)
+    counts_form = S is None
+    if counts_form:
+        S_buf = torch.empty(nsys, dtype=torch.uint8)
+        s_kind = abi.GSB_CODES
+    else:
+        if not (isinstance(S, torch.Tensor) and S.dtype == torch.uint8 and S.device.type == "cpu"):
+            raise ArgumentError("S must be a (nsys, 72) uint8 host tensor")
+        if S.numel() != nsys * 72:
+            raise DimensionMismatch(f"status vector length {S.numel() // 72} does not match batch length {nsys}")
+        S_buf, s_kind = S, abi.GSB_STATUS64
+    gm, go = method.to_abi(), opt.to_abi()
+    if nsys == 0:
+        return ReturnCodeCounts(0, 0, 0, 0, 0, 0) if counts_form else S
+    device = torch.device(device or "cuda")
+    lib = abi.load_library()
+    sh = prob.shared_device(device)
+    gp = prob.to_abi(None if sh is None else sh.data_ptr())
+    tally = abi.GsbTally()
+    with torch.cuda.device(device):
+        _raise_for(lib.gsb_solve_batch_host(
+            ctypes.byref(gp), ctypes.byref(gm), ctypes.byref(go), X.data_ptr(), S_buf.data_ptr(),
+            s_kind, Pt.data_ptr(), nsys, int(chunk), ctypes.byref(tally)), lib)
     if counts_form:
         return ReturnCodeCounts(*[int(c) for c in tally.counts])
     return S

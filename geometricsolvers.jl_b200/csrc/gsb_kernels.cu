@@ -912,3 +912,127 @@ int gsb_solve_batch_uneven(const GsbMethod* method, const GsbOptions* opt, doubl
 }
 
 }  // extern "C"
+
+// ─── batches in host memory ─────────────────────────────────────────────────────────────────
+//
+// The batch streams through the device in chunks over three streams: while chunk k solves, the
+// inputs of chunk k+1 arrive and the results of chunk k-1 leave, so the copies in both
+// directions and the solves overlap (page-locked host memory lets the copies run asynchronously).
+// Three staging slots per device are kept between calls.
+
+namespace {
+
+constexpr int kSlots = 3;
+
+struct HostPipe {
+    double* x[kSlots] = {};
+    double* p[kSlots] = {};
+    unsigned char* s[kSlots] = {};
+    int64_t cap_x = 0, cap_p = 0, cap_s = 0;  // bytes per slot
+    unsigned long long* tally = nullptr;
+    cudaStream_t h2d = nullptr, comp = nullptr, d2h = nullptr;
+    cudaEvent_t in[kSlots] = {}, solved[kSlots] = {}, out[kSlots] = {};
+};
+std::mutex g_pipe_mu;
+HostPipe g_pipe[64];
+
+int pipe_grow(void** buf, int64_t& cap, int64_t bytes) {
+    if (cap >= bytes) return 0;
+    if (*buf) cudaFree(*buf);
+    *buf = nullptr;
+    cap = 0;
+    if (int rc = cuda_err(cudaMalloc(buf, bytes), "cudaMalloc")) return rc;
+    cap = bytes;
+    return 0;
+}
+
+int pipe_setup(HostPipe& hp, int64_t xb, int64_t pb, int64_t sb) {
+    if (!hp.h2d) {
+        for (cudaStream_t* st : {&hp.h2d, &hp.comp, &hp.d2h})
+            if (int rc = cuda_err(cudaStreamCreateWithFlags(st, cudaStreamNonBlocking), "stream")) return rc;
+        for (int k = 0; k < kSlots; ++k)
+            for (cudaEvent_t* ev : {&hp.in[k], &hp.solved[k], &hp.out[k]})
+                if (int rc = cuda_err(cudaEventCreateWithFlags(ev, cudaEventDisableTiming), "event"))
+                    return rc;
+        if (int rc = cuda_err(cudaMalloc(&hp.tally, 6 * sizeof(unsigned long long)), "cudaMalloc"))
+            return rc;
+    }
+    int64_t cx = hp.cap_x, cp = hp.cap_p, cs = hp.cap_s;
+    for (int k = 0; k < kSlots; ++k) {
+        int64_t a = cx, b = cp, c = cs;
+        if (int rc = pipe_grow(reinterpret_cast<void**>(&hp.x[k]), a, xb)) return rc;
+        if (int rc = pipe_grow(reinterpret_cast<void**>(&hp.p[k]), b, pb)) return rc;
+        if (int rc = pipe_grow(reinterpret_cast<void**>(&hp.s[k]), c, sb)) return rc;
+        if (k == kSlots - 1) {
+            hp.cap_x = a;
+            hp.cap_p = b;
+            hp.cap_s = c;
+        }
+    }
+    return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int gsb_solve_batch_host(const GsbProblem* prob, const GsbMethod* method, const GsbOptions* opt,
+                         double* X, void* S, int32_t s_kind, const double* P, int64_t nsys,
+                         int64_t chunk, GsbTally* tally) {
+    g_err.clear();
+    if (!prob || !method || !opt) return set_err(GSB_ERR_ARGUMENT, "null problem, method or options");
+    if (nsys < 0) return set_err(GSB_ERR_DIMENSION, "negative batch length");
+    if (int rc = check_options(opt)) return rc;
+    if (int rc = check_method(method)) return rc;
+    const int64_t np = param_count(prob);
+    if (np < 0) return set_err(GSB_ERR_ARGUMENT, "unknown family or size");
+    if (s_kind != GSB_STATUS64 && s_kind != GSB_CODES) return set_err(GSB_ERR_ARGUMENT, "s_kind");
+    if (chunk < 0) return set_err(GSB_ERR_ARGUMENT, "negative chunk");
+    if (tally) std::memset(tally, 0, sizeof(*tally));
+    if (nsys == 0) return 0;
+    if (!X || !S || !P) return set_err(GSB_ERR_ARGUMENT, "null X, S or P");
+    const int64_t n = prob->n;
+    const int64_t sbytes = s_kind == GSB_STATUS64 ? 72 : 1;
+    if (chunk == 0) chunk = 131072;
+    if (chunk > nsys) chunk = nsys;
+    int dev = 0;
+    if (int rc = cuda_err(cudaGetDevice(&dev), "cudaGetDevice")) return rc;
+    if (dev < 0 || dev >= 64) return set_err(GSB_ERR_CUDA, "device index out of range");
+    std::lock_guard<std::mutex> lk(g_pipe_mu);
+    HostPipe& hp = g_pipe[dev];
+    if (int rc = pipe_setup(hp, chunk * n * 8, chunk * np * 8, chunk * sbytes)) return rc;
+    if (int rc = cuda_err(cudaMemsetAsync(hp.tally, 0, 6 * sizeof(unsigned long long), hp.comp), "memset"))
+        return rc;
+    const int64_t nchunks = (nsys + chunk - 1) / chunk;
+    for (int64_t c = 0; c < nchunks; ++c) {
+        const int k = (int)(c % kSlots);
+        const int64_t first = c * chunk;
+        const int64_t len = std::min(chunk, nsys - first);
+        // the slot's previous results have left before its new inputs arrive
+        if (c >= kSlots) cudaStreamWaitEvent(hp.h2d, hp.out[k], 0);
+        cudaMemcpyAsync(hp.x[k], X + first * n, len * n * 8, cudaMemcpyHostToDevice, hp.h2d);
+        cudaMemcpyAsync(hp.p[k], P + first * np, len * np * 8, cudaMemcpyHostToDevice, hp.h2d);
+        cudaEventRecord(hp.in[k], hp.h2d);
+        cudaStreamWaitEvent(hp.comp, hp.in[k], 0);
+        if (int rc = launch_solve(prob, method, opt, hp.x[k], GSB_AOS, hp.s[k], s_kind, hp.p[k],
+                                  GSB_AOS, nullptr, 0, len, hp.comp, tally ? hp.tally : nullptr))
+            return rc;
+        cudaEventRecord(hp.solved[k], hp.comp);
+        cudaStreamWaitEvent(hp.d2h, hp.solved[k], 0);
+        cudaMemcpyAsync(X + first * n, hp.x[k], len * n * 8, cudaMemcpyDeviceToHost, hp.d2h);
+        cudaMemcpyAsync(static_cast<unsigned char*>(S) + first * sbytes, hp.s[k], len * sbytes,
+                        cudaMemcpyDeviceToHost, hp.d2h);
+        cudaEventRecord(hp.out[k], hp.d2h);
+    }
+    unsigned long long h[6] = {};
+    if (tally) cudaMemcpyAsync(h, hp.tally, sizeof(h), cudaMemcpyDeviceToHost, hp.comp);
+    cudaError_t e = cudaStreamSynchronize(hp.comp);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(hp.d2h);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(hp.h2d);
+    if (int rc = cuda_err(e, "host batch")) return rc;
+    if (tally)
+        for (int c = 0; c < 6; ++c) tally->counts[c] = (int64_t)h[c];
+    return 0;
+}
+
+}  // extern "C"

@@ -269,6 +269,17 @@ GSB_API int gsb_solve_batch_counts_noalloc(const GsbProblem* prob, const GsbMeth
                                            const int64_t* order, int32_t order_base,
                                            int64_t nsys, void* stream, GsbTally* tally);
 
+/* A batch whose X, S and P live in host memory (AoS layouts; page-locked memory lets the copies
+ * overlap). No counterpart in the reference's device path: the call streams the batch through
+ * the device in chunks of `chunk` systems (0: 131,072), on three streams, so that the copy of
+ * chunk k+1's inputs, the solve of chunk k and the copy back of chunk k-1's iterates and statuses
+ * overlap. `prob->shared` must still be a device pointer. Three device staging slots are
+ * allocated on the first call on a device and kept. The call returns when every result is in
+ * host memory; tally as in gsb_solve_batch. */
+GSB_API int gsb_solve_batch_host(const GsbProblem* prob, const GsbMethod* method,
+                                 const GsbOptions* opt, double* X, void* S, int32_t s_kind,
+                                 const double* P, int64_t nsys, int64_t chunk, GsbTally* tally);
+
 /* ─── ragged batches: systems of different sizes in one call ───────────────────────────────
  *
  * No counterpart in the reference, whose solve_batch! takes one size per call: a batch of

@@ -122,10 +122,11 @@ __device__ __forceinline__ void tally_code(unsigned long long* tally, int code) 
     }
 }
 
-// Stage the contiguous AoS parameter chunk of a CTA (`rows` blocks of NP doubles from src) into
-// rows of stride RS in shared memory. Each thread issues all of its loads before any store, in
-// batches of 16, so that the HBM round trips of one thread overlap instead of following one
-// another.
+// Stage the contiguous AoS parameter chunk of a CTA (`rows_left` blocks of NP doubles from src,
+// at most ROWS) into rows of stride RS in shared memory (entry k of a block at `place(k)`), as
+// asynchronous 8-byte global-to-shared copies: the warp's lanes copy consecutive doubles
+// (coalesced), every copy of a thread is in flight at once and holds no register, and the
+// thread waits once for all of them. The caller's barrier then publishes the rows to the CTA.
 struct IdentityPlace {
     __device__ __forceinline__ int operator()(int k) const { return k; }
 };
@@ -134,26 +135,13 @@ template <int NP, int RS, int ROWS, class Place = IdentityPlace>
 __device__ __forceinline__ void stage_aos(double* smem, const double* src, int64_t rows_left, int tid,
                                           Place place = Place()) {
     constexpr int TOTAL = ROWS * NP;
-    constexpr int PER = (TOTAL + kThreads - 1) / kThreads;
-    constexpr int BATCH = 16;
     const int total = rows_left < ROWS ? (int)rows_left * NP : TOTAL;
-#pragma unroll
-    for (int b0 = 0; b0 < PER; b0 += BATCH) {
-        double v[BATCH];
-#pragma unroll
-        for (int b = 0; b < BATCH; ++b) {
-            const int q = (b0 + b) * kThreads + tid;
-            v[b] = (b0 + b < PER && q < total) ? __ldg(src + q) : 0.0;
-        }
-#pragma unroll
-        for (int b = 0; b < BATCH; ++b) {
-            const int q = (b0 + b) * kThreads + tid;
-            if (b0 + b < PER && q < total) {
-                const int s = q / NP;
-                smem[s * RS + place(q - s * NP)] = v[b];
-            }
-        }
+    for (int q = tid; q < total; q += kThreads) {
+        const int s = q / NP;
+        const unsigned dst = smem_addr(smem + s * RS + place(q - s * NP));
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(dst), "l"(src + q) : "memory");
     }
+    asm volatile("cp.async.wait_all;" ::: "memory");
 }
 
 // Resident 128-thread blocks per SM that the register allocation must allow, by system size.

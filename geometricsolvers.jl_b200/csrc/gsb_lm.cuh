@@ -121,6 +121,14 @@ __device__ __forceinline__ void givens(double f, double g, double& cs, double& s
     const double scale = jmax(fabs(f), fabs(g));
     if (scale >= kSafmx2 || scale <= kSafmn2) {
         givens_rescaled<F>(f, g, cs, sn, r);
+    } else if constexpr (F) {
+        // fused arithmetic: one reciprocal square root in place of a square root and two
+        // divisions (the rotation agrees with the reference's to rounding)
+        const double q = A::madd(g, g, A::mul(f, f));
+        const double ri = rsqrt(q);
+        r = A::mul(q, ri);
+        cs = A::mul(f, ri);
+        sn = A::mul(g, ri);
     } else {
         r = __dsqrt_rn(A::madd(g, g, A::mul(f, f)));
         cs = __ddiv_rn(f, r);
@@ -331,12 +339,14 @@ template <class Fam, bool F> struct LMSolver {
         for (int k = 0; k < N * N; ++k) R[k] = q.R[k];
 #pragma unroll
         for (int k = 0; k < N; ++k) c[k] = q.c[k];
-#pragma unroll
+        // the damping rows sqrt(mu) e_j, one at a time (a runtime loop over one copy of the
+        // row fold, which skips the columns before j)
+        const double sq1 = A::mul(sq, 1.0);
+#pragma unroll 1
         for (int j = 0; j < N; ++j) {
             double w[N];
 #pragma unroll
-            for (int k = 0; k < N; ++k) w[k] = 0.0;
-            w[j] = A::mul(sq, 1.0);
+            for (int k = 0; k < N; ++k) w[k] = k == j ? sq1 : 0.0;
             fold_row<F, N>(R, c, w, 0.0, j);
         }
 #pragma unroll

@@ -765,6 +765,24 @@ def run_workload(args):
         solved_frac = float(np.mean(ok))
         with Clocks(0) as clk:
             ms = _events_ms(step, args.steps, args.warmup, stream)
+            if args.workload == "c2":
+                # the mixed form: FP32 stacked factor with FP64 refinement
+                m32 = G.Newton(linsolve=G.QRFactorization("float32"),
+                               globalization=G.LevenbergMarquardt())
+
+                def step32():
+                    X.copy_(X0)
+                    G.solve_batch(X, S, prob, m32, ps, options=opts)
+
+                ms32 = _events_ms(step32, args.steps, args.warmup, stream)
+                step32()
+                st32 = G.statuses(S)
+                fr32 = np.abs(st32["fnorm"][:ns] - so["fnorm"]) / np.maximum(so["fnorm"], 1e-300)
+                ok32 = (st32["code"][:ns] == so["code"]) & (
+                    fr32 <= np.where(so["code"] == 0, 1e-10, 1e-9))
+                forms["fp32_qr_refinement"] = {
+                    "systems_per_s": float(np.mean(ok32)) * nsys / (ms32 * 1e-3), "ms_per_step": ms32,
+                    "solved_fraction": float(np.mean(ok32)), "oracle_checked_systems": ns}
         clocks = clk.summary()
         value = solved_frac * nsys / (ms * 1e-3)
         # the solve alone: the step minus the copy of the start iterates
@@ -793,6 +811,12 @@ def run_workload(args):
                          "oracle_checked_systems": ns}
         launches = args.steps
         chosen = "fp64"
+        if "fp32_qr_refinement" in forms and forms["fp32_qr_refinement"]["systems_per_s"] > value:
+            chosen = "fp32_qr_refinement"
+            value = forms[chosen]["systems_per_s"]
+            ms = forms[chosen]["ms_per_step"]
+        if args.workload == "c2":
+            forms["chosen_over_plain"] = value / forms["fp64"]["systems_per_s"]
     else:
         from workloads import c4
 

@@ -254,7 +254,7 @@ __global__ void __launch_bounds__(kThreads) team_kernel(const __grid_constant__ 
 
 // The least-squares form: one Levenberg–Marquardt solve per thread. Shared memory holds each
 // system's M observations (odd row stride) and, after the rows, the M abscissae of the batch.
-template <class Fam, bool F>
+template <class Fam, bool F, bool Mixed>
 __global__ void __launch_bounds__(kThreads, 3) lm_kernel(const __grid_constant__ GsbMethod m,
                                  const __grid_constant__ GsbOptions o,
                                  const __grid_constant__ Launch L) {
@@ -286,7 +286,7 @@ __global__ void __launch_bounds__(kThreads, 3) lm_kernel(const __grid_constant__
 #pragma unroll
     for (int k = 0; k < N; ++k)
         x[k] = L.x_layout == GSB_SOA ? L.X[(int64_t)k * L.nsys + idx] : L.X[idx * N + k];
-    LMSolver<Fam, F> sv(fam, m, o);
+    LMSolver<Fam, F, Mixed> sv(fam, m, o);
     double gr;
     DevStatus s = sv.solve(x, gr);
 #pragma unroll
@@ -372,9 +372,9 @@ template <class Fam, bool F, bool Mixed, bool PlainRef> KernelEntry* entry() {
     return &e;
 }
 
-template <class Fam, bool F> KernelEntry* lm_entry() {
+template <class Fam, bool F, bool Mixed> KernelEntry* lm_entry() {
     constexpr int RS = (Fam::M % 2 == 1) ? Fam::M : Fam::M + 1;
-    static KernelEntry e{lm_kernel<Fam, F>, nullptr, kThreads * RS + Fam::M, kThreads, {}};
+    static KernelEntry e{lm_kernel<Fam, F, Mixed>, nullptr, kThreads * RS + Fam::M, kThreads, {}};
     return &e;
 }
 

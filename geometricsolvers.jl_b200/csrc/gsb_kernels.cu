@@ -174,7 +174,7 @@ GSB_DECLARE_ENTRY(hetero6);
 GSB_DECLARE_ENTRY(coupled2);
 GSB_DECLARE_TEAM(cubic6);
 GSB_DECLARE_TEAM(cubic8);
-KernelEntry* lm_expsum3_64(bool fused);
+KernelEntry* lm_expsum3_64(bool fused, bool mixed);
 KernelEntry* warp_cubic12(bool fused, bool mixed, bool refine, int T);
 KernelEntry* warp_cubic16(bool fused, bool mixed, bool refine, int T);
 KernelEntry* warp_cubic24(bool fused, bool mixed, bool refine, int T);
@@ -319,14 +319,14 @@ int launch_solve(const GsbProblem* prob, const GsbMethod* method, const GsbOptio
         if (!lm)
             return set_err(GSB_ERR_UNSUPPORTED,
                            "the least-squares batch kernel runs the LevenbergMarquardt step");
-        if (mixed)
+        if (method->refinement == GSB_REFINEMENT)
             return set_err(GSB_ERR_UNSUPPORTED,
-                           "LevenbergMarquardt factors in the working precision");
+                           "Newton with a LevenbergMarquardt globalization takes no refinement");
         if (method->threads_per_system > 1)
             return set_err(GSB_ERR_UNSUPPORTED, "one thread per least-squares system");
         if (prob->m != 64) return set_err(GSB_ERR_UNSUPPORTED, "no batch kernel for this m");
         if (!prob->shared) return set_err(GSB_ERR_ARGUMENT, "the abscissae t are missing");
-        ke = lm_expsum3_64(fused);
+        ke = lm_expsum3_64(fused, mixed);
     } else {
         if (lm)
             return set_err(GSB_ERR_UNSUPPORTED,
@@ -465,14 +465,14 @@ int gsb_solve_batch(const GsbProblem* prob, const GsbMethod* method, const GsbOp
         if (!lm)
             return set_err(GSB_ERR_UNSUPPORTED,
                            "the least-squares batch kernel runs the LevenbergMarquardt step");
-        if (mixed)
+        if (method->refinement == GSB_REFINEMENT)
             return set_err(GSB_ERR_UNSUPPORTED,
-                           "LevenbergMarquardt factors in the working precision");
+                           "Newton with a LevenbergMarquardt globalization takes no refinement");
         if (method->threads_per_system > 1)
             return set_err(GSB_ERR_UNSUPPORTED, "one thread per least-squares system");
         if (prob->m != 64) return set_err(GSB_ERR_UNSUPPORTED, "no batch kernel for this m");
         if (!prob->shared) return set_err(GSB_ERR_ARGUMENT, "the abscissae t are missing");
-        ke = lm_expsum3_64(fused);
+        ke = lm_expsum3_64(fused, mixed);
     } else {
         if (lm)
             return set_err(GSB_ERR_UNSUPPORTED,

@@ -141,32 +141,69 @@ __device__ __forceinline__ void givens(double f, double g, double& cs, double& s
     }
 }
 
-// (u, v) <- (c u + s v, -s u + c v)
-template <bool F> __device__ __forceinline__ void rotate(double cs, double sn, double& u, double& v) {
+// The FP32 rotation of the FP32 stacked factor (the mixed form): one reciprocal square root;
+// arguments whose squares leave the FP32 range take the FP64 rotation.
+template <bool F>
+__device__ __forceinline__ void givens(float f, float g, float& cs, float& sn, float& r) {
     using A = Arith<F>;
-    const double nu = A::madd(cs, u, A::mul(sn, v));
-    const double nv = A::madd(cs, v, A::mul(-sn, u));
+    if (g == 0.0f) {
+        cs = 1.0f;
+        sn = 0.0f;
+        r = f;
+        return;
+    }
+    if (f == 0.0f) {
+        cs = 0.0f;
+        sn = 1.0f;
+        r = g;
+        return;
+    }
+    const float scale = fmaxf(fabsf(f), fabsf(g));
+    if (!(scale < 1.0e18f && scale > 1.0e-18f)) {
+        double c2, s2, r2;
+        givens<F>((double)f, (double)g, c2, s2, r2);
+        cs = (float)c2;
+        sn = (float)s2;
+        r = (float)r2;
+        return;
+    }
+    const float q = A::madd(g, g, A::mul(f, f));
+    const float ri = rsqrtf(q);
+    r = A::mul(q, ri);
+    cs = A::mul(f, ri);
+    sn = A::mul(g, ri);
+    if (fabsf(f) > fabsf(g) && cs < 0.0f) {
+        cs = -cs;
+        sn = -sn;
+        r = -r;
+    }
+}
+
+// (u, v) <- (c u + s v, -s u + c v)
+template <bool F, class T> __device__ __forceinline__ void rotate(T cs, T sn, T& u, T& v) {
+    using A = Arith<F>;
+    const T nu = A::madd(cs, u, A::mul(sn, v));
+    const T nv = A::madd(cs, v, A::mul(-sn, u));
     u = nu;
     v = nv;
 }
 
 // Fold the row (w | wr) into the triangle (R, c) from column k0 on: the row loop of
 // lm_qr_factor! and of the damping rows. Returns the residual component left in wr.
-template <bool F, int N>
-__device__ __forceinline__ double fold_row(double (&R)[N * N], double (&c)[N], double (&w)[N],
-                                           double wr, int k0) {
+template <bool F, int N, class T>
+__device__ __forceinline__ T fold_row(T (&R)[N * N], T (&c)[N], T (&w)[N], T wr, int k0) {
 #pragma unroll
     for (int k = 0; k < N; ++k) {
         if (k < k0) continue;
-        const double b = w[k];
-        if (b == 0.0) continue;
-        double cs, sn, rv;
+        const T b = w[k];
+        if (b == T(0)) continue;
+        T cs, sn, rv;
         givens<F>(R[k + k * N], b, cs, sn, rv);
         R[k + k * N] = rv;
-        w[k] = 0.0;
+        w[k] = T(0);
 #pragma unroll
-        for (int l = k + 1; l < N; ++l) rotate<F>(cs, sn, R[k + l * N], w[l]);
-        rotate<F>(cs, sn, c[k], wr);
+        for (int l = k + 1; l < N; ++l) rotate<F, T>(cs, sn, R[k + l * N], w[l]);
+        rotate<F, T>(cs, sn, c[k], wr);
     }
     return wr;
 }
@@ -179,7 +216,22 @@ template <int N> struct StackedQR {
     double rest2;
 };
 
-template <class Fam, bool F> struct LMSolver {
+// The mixed form's factorisation of one Jacobian pass: the FP32 stacked triangle, and in FP64
+// the Gram matrix J'J (upper triangle, row by row) and the gradient J'F, from which the
+// refinement's residuals and the predicted reduction are formed.
+template <int N> struct MixedQR {
+    float R[N * N];
+    float c[N];
+    double G[N * (N + 1) / 2];
+    double g[N];
+    bool fits;  // every row entry within the FP32 range
+};
+
+template <int N> __host__ __device__ constexpr int gram_index(int k, int l) {
+    return k * N - k * (k - 1) / 2 + (l - k);  // k <= l
+}
+
+template <class Fam, bool F, bool Mixed = false> struct LMSolver {
     static constexpr int N = Fam::N, M = Fam::M;
     using A = Arith<F>;
     const Fam& fam;
@@ -227,10 +279,30 @@ template <class Fam, bool F> struct LMSolver {
     template <bool QR>
     __device__ void jacobian_pass(const double (&x)[N], double fnorm, State& st, StackedQR<N>& q,
                                   bool& finite) const {
+        jacobian_pass_impl<QR ? 1 : 0>(x, fnorm, st, &q, nullptr, finite);
+    }
+    __device__ void jacobian_pass_mixed(const double (&x)[N], double fnorm, State& st,
+                                        MixedQR<N>& q, bool& finite) const {
+        jacobian_pass_impl<2>(x, fnorm, st, nullptr, &q, finite);
+    }
+
+    // Mode 0: the diagnostics only; 1: and the FP64 stacked factor; 2: and the FP32 stacked
+    // factor with the FP64 Gram matrix and gradient (the mixed form).
+    template <int Mode>
+    __device__ void jacobian_pass_impl(const double (&x)[N], double fnorm, State& st,
+                                       StackedQR<N>* qp, MixedQR<N>* qmp, bool& finite) const {
+        StackedQR<N>& q = *qp;   // bound only where Mode == 1 reads it
+        MixedQR<N>& qm = *qmp;   // bound only where Mode == 2 reads it
+        constexpr bool QR = Mode == 1;
         double g[N];
         double js = 0.0, jm = 0.0;
         bool fin = true;
+        bool fits = true;
         double rest2 = 0.0;
+        if constexpr (Mode == 2) {
+#pragma unroll
+            for (int k = 0; k < N * (N + 1) / 2; ++k) qm.G[k] = 0.0;
+        }
         // rows 0..N-1: the block of R0 and c0, reduced column by column
 #pragma unroll
         for (int i = 0; i < N; ++i) {
@@ -243,8 +315,35 @@ template <class Fam, bool F> struct LMSolver {
                 jm = (i == 0 && k == 0) ? fabs(J[k]) : jmax(jm, fabs(J[k]));
                 fin = fin && isfin(J[k]);
                 if constexpr (QR) q.R[i + k * N] = J[k];
+                if constexpr (Mode == 2) {
+                    qm.R[i + k * N] = (float)J[k];
+                    fits = fits && isfinite(qm.R[i + k * N]);
+#pragma unroll
+                    for (int l = k; l < N; ++l)
+                        qm.G[gram_index<N>(k, l)] = A::madd(J[k], J[l], qm.G[gram_index<N>(k, l)]);
+                }
             }
             if constexpr (QR) q.c[i] = -r;
+            if constexpr (Mode == 2) {
+                qm.c[i] = -(float)r;
+                fits = fits && isfinite(qm.c[i]);
+            }
+        }
+        if constexpr (Mode == 2) {
+#pragma unroll
+            for (int j = 0; j < N; ++j)
+#pragma unroll
+                for (int i = j + 1; i < N; ++i) {
+                    const float b = qm.R[i + j * N];
+                    if (b == 0.0f) continue;
+                    float cs, sn, rv;
+                    givens<F>(qm.R[j + j * N], b, cs, sn, rv);
+                    qm.R[j + j * N] = rv;
+                    qm.R[i + j * N] = 0.0f;
+#pragma unroll
+                    for (int k = j + 1; k < N; ++k) rotate<F, float>(cs, sn, qm.R[j + k * N], qm.R[i + k * N]);
+                    rotate<F, float>(cs, sn, qm.c[j], qm.c[i]);
+                }
         }
         if constexpr (QR) {
 #pragma unroll
@@ -258,8 +357,8 @@ template <class Fam, bool F> struct LMSolver {
                     q.R[j + j * N] = rv;
                     q.R[i + j * N] = 0.0;
 #pragma unroll
-                    for (int k = j + 1; k < N; ++k) rotate<F>(cs, sn, q.R[j + k * N], q.R[i + k * N]);
-                    rotate<F>(cs, sn, q.c[j], q.c[i]);
+                    for (int k = j + 1; k < N; ++k) rotate<F, double>(cs, sn, q.R[j + k * N], q.R[i + k * N]);
+                    rotate<F, double>(cs, sn, q.c[j], q.c[i]);
                 }
         }
         // rows N..M-1, each rotated into the triangle as it is generated
@@ -275,11 +374,33 @@ template <class Fam, bool F> struct LMSolver {
                 fin = fin && isfin(J[k]);
             }
             if constexpr (QR) {
-                const double wr = fold_row<F, N>(q.R, q.c, J, -r, 0);
+                const double wr = fold_row<F, N, double>(q.R, q.c, J, -r, 0);
                 rest2 = A::madd(wr, wr, rest2);
+            }
+            if constexpr (Mode == 2) {
+                float Jf[N];
+#pragma unroll
+                for (int k = 0; k < N; ++k) {
+                    Jf[k] = (float)J[k];
+                    fits = fits && isfinite(Jf[k]);
+#pragma unroll
+                    for (int l = k; l < N; ++l)
+                        qm.G[gram_index<N>(k, l)] = A::madd(J[k], J[l], qm.G[gram_index<N>(k, l)]);
+                }
+                const float rf = -(float)r;
+                fits = fits && isfinite(rf);
+                fold_row<F, N, float>(qm.R, qm.c, Jf, rf, 0);
             }
         }
         if constexpr (QR) q.rest2 = rest2;
+        if constexpr (Mode == 2) {
+#pragma unroll
+            for (int k = 0; k < N; ++k) {
+                qm.g[k] = g[k];
+                fits = fits && isfinite(qm.R[k + k * N]);
+            }
+            qm.fits = fits;
+        }
         finite = fin;
         // ‖J‖_F: rnorm over the M N entries, with its scaled fallback
         double jnorm;
@@ -347,7 +468,7 @@ template <class Fam, bool F> struct LMSolver {
             double w[N];
 #pragma unroll
             for (int k = 0; k < N; ++k) w[k] = k == j ? sq1 : 0.0;
-            fold_row<F, N>(R, c, w, 0.0, j);
+            fold_row<F, N, double>(R, c, w, 0.0, j);
         }
 #pragma unroll
         for (int i = 0; i < N; ++i) d[i] = 0.0;
@@ -402,26 +523,131 @@ template <class Fam, bool F> struct LMSolver {
         return pred;
     }
 
-    // The LevenbergMarquardt step, newton.jl:1897-1971.
-    __device__ void step(State& st, double (&x)[N], StepInfo& info) const {
-        const double fnorm = st.fnorm;
-        double mu = st.mu;
-        if (!isfin(mu)) {
-            info = {NONFINITE, fnorm, 0.0, 0, false, false, false};
-            return;
+    // The mixed form's trial: the damped FP32 triangle and back substitution, then refinement
+    // of d against the FP64 residual of the damped normal equations,
+    // r = -J'F - (J'J + damp I) d, solved on the same triangle (R' R = J'J + damp I).
+    __device__ bool trial(const MixedQR<N>& q, double mu, double (&d)[N]) const {
+        const double damp = mu < 4.0 * kEps ? 0.0 : mu;
+        const double sq = __dsqrt_rn(damp);
+        if (!isfin(sq) || !isfin(A::mul(sq, 1.0))) {
+#pragma unroll
+            for (int i = 0; i < N; ++i) d[i] = 0.0;
+            return false;
         }
-        if (fnorm == 0.0) {
-            info = {SUCCESS, 0.0, 0.0, 0, false, false, false};
-            return;
+        float R[N * N], c[N];
+#pragma unroll
+        for (int k = 0; k < N * N; ++k) R[k] = q.R[k];
+#pragma unroll
+        for (int k = 0; k < N; ++k) c[k] = q.c[k];
+        const float sqf = (float)A::mul(sq, 1.0);
+#pragma unroll 1
+        for (int j = 0; j < N; ++j) {
+            float w[N];
+#pragma unroll
+            for (int k = 0; k < N; ++k) w[k] = k == j ? sqf : 0.0f;
+            fold_row<F, N, float>(R, c, w, 0.0f, j);
         }
-        const double mu_min_eff = jmax(m.lm_mu_min, 4.0 * kEps);
-        StackedQR<N> q;
-        bool finite;
-        jacobian_pass<true>(x, fnorm, st, q, finite);
-        if (!finite) {
-            info = {NONFINITE, fnorm, 0.0, 0, false, false, false};
-            return;
+        float df[N];
+        bool ok = true;
+#pragma unroll
+        for (int i = N - 1; i >= 0; --i) {
+            float s = c[i];
+#pragma unroll
+            for (int j = i + 1; j < N; ++j) s = Arith<F>::msub(R[i + j * N], df[j], s);
+            ok = ok && R[i + i * N] != 0.0f && isfinite(R[i + i * N]);
+            df[i] = ok ? s / R[i + i * N] : 0.0f;
         }
+#pragma unroll
+        for (int i = 0; i < N; ++i) {
+            d[i] = (double)df[i];
+            ok = ok && isfin(d[i]);
+        }
+        if (!ok) return false;
+        // refinement passes (the Refinement parameters of the method: eta, maxiter)
+        double r[N];
+        auto residual = [&](const double (&v)[N], double (&out)[N]) {
+#pragma unroll
+            for (int a = 0; a < N; ++a) {
+                double t = A::madd(damp, v[a], q.g[a]);
+#pragma unroll
+                for (int b = 0; b < N; ++b)
+                    t = A::madd(q.G[a <= b ? gram_index<N>(a, b) : gram_index<N>(b, a)], v[b], t);
+                out[a] = -t;
+            }
+        };
+        residual(d, r);
+        const double thr = A::mul(jmax(m.refine_eta, kSqrtEps), rnorm<F, N>(q.g));
+        double rprev = rnorm<F, N>(r);
+        for (int it = 0; it < m.refine_maxiter && isfin(rprev) && rprev > thr; ++it) {
+            double sc = fabs(r[0]);
+#pragma unroll
+            for (int a = 1; a < N; ++a) sc = jmax(sc, fabs(r[a]));
+            if (!(sc > 0.0) || !isfin(sc)) break;
+            // R' y = r / sc (forward), then R z = y (back), in FP32
+            float y[N];
+#pragma unroll
+            for (int a = 0; a < N; ++a) {
+                float t = (float)(r[a] / sc);
+#pragma unroll
+                for (int b = 0; b < a; ++b) t = Arith<F>::msub(R[b + a * N], y[b], t);
+                y[a] = t / R[a + a * N];
+            }
+#pragma unroll
+            for (int a = N - 1; a >= 0; --a) {
+                float t = y[a];
+#pragma unroll
+                for (int b = a + 1; b < N; ++b) t = Arith<F>::msub(R[a + b * N], y[b], t);
+                y[a] = t / R[a + a * N];
+            }
+            double dc[N], rc[N];
+#pragma unroll
+            for (int a = 0; a < N; ++a) dc[a] = A::madd((double)y[a], sc, d[a]);
+            residual(dc, rc);
+            const double rn = rnorm<F, N>(rc);
+            if (!(rn < rprev)) break;
+#pragma unroll
+            for (int a = 0; a < N; ++a) {
+                d[a] = dc[a];
+                r[a] = rc[a];
+            }
+            rprev = rn;
+        }
+#pragma unroll
+        for (int i = 0; i < N; ++i)
+            if (!isfin(d[i])) return false;
+        return true;
+    }
+
+    // The predicted reduction from the FP64 Gram matrix and gradient: -2 g'd - d'G d (the
+    // reference's -2 F'(J d) - |J d|^2 in exact arithmetic); its fallback |F + J d|^2 =
+    // |F|^2 + 2 g'd + d'G d.
+    __device__ double predicted(const MixedQR<N>& q, const double (&d)[N], double fnorm) const {
+        double gd = A::mul(q.g[0], d[0]);
+#pragma unroll
+        for (int a = 1; a < N; ++a) gd = A::madd(q.g[a], d[a], gd);
+        double dGd = 0.0;
+#pragma unroll
+        for (int a = 0; a < N; ++a) {
+            double t = 0.0;
+#pragma unroll
+            for (int b = 0; b < N; ++b)
+                t = A::madd(q.G[a <= b ? gram_index<N>(a, b) : gram_index<N>(b, a)], d[b], t);
+            dGd = A::madd(d[a], t, dGd);
+        }
+        double pred = A::sub(A::mul(-2.0, gd), dGd);
+        if (pred <= 0.0) {
+            const double fl2 = A::add(A::madd(2.0, gd, A::mul(fnorm, fnorm)), dGd);
+            const double fl = __dsqrt_rn(fl2 > 0.0 ? fl2 : 0.0);
+            pred = A::mul(A::sub(fnorm, fl), A::add(fnorm, fl));
+        }
+        return pred;
+    }
+
+    // The trials of one step on a factorisation (newton.jl:1906-1971): damped solve, predicted
+    // and actual reduction, the gain ratio; mu grows after each rejected trial.
+    template <class Q>
+    __device__ void trials(const Q& q, State& st, double (&x)[N], StepInfo& info, double fnorm,
+                           double mu, double mu_min_eff, bool promoted) const {
         int failures = 0;
         while (true) {
             double d[N];
@@ -444,7 +670,7 @@ template <class Fam, bool F> struct LMSolver {
                         st.fnorm = fnp;
                         st.fmax = fmaxp;
                         st.mu = mu_next;
-                        info = {SUCCESS, fnp, stepnorm, failures, false, limited, false};
+                        info = {SUCCESS, fnp, stepnorm, failures, promoted, limited, false};
                         return;
                     }
                 }
@@ -453,10 +679,46 @@ template <class Fam, bool F> struct LMSolver {
             mu = jmax(A::mul(mu, m.lm_mu_increase), mu_min_eff);
             if (!isfin(mu) || mu > m.lm_mu_max) {
                 st.mu = jmin(mu, kFloatmax);
-                info = {STALLED, fnorm, 0.0, failures, false, false, false};
+                info = {STALLED, fnorm, 0.0, failures, promoted, false, false};
                 return;
             }
         }
+    }
+
+    // The LevenbergMarquardt step, newton.jl:1897-1971. The mixed form factors in FP32 and
+    // refines in FP64; a step whose rows leave the FP32 range is taken in FP64 (`promoted`).
+    __device__ void step(State& st, double (&x)[N], StepInfo& info) const {
+        const double fnorm = st.fnorm;
+        const double mu = st.mu;
+        if (!isfin(mu)) {
+            info = {NONFINITE, fnorm, 0.0, 0, false, false, false};
+            return;
+        }
+        if (fnorm == 0.0) {
+            info = {SUCCESS, 0.0, 0.0, 0, false, false, false};
+            return;
+        }
+        const double mu_min_eff = jmax(m.lm_mu_min, 4.0 * kEps);
+        bool finite;
+        if constexpr (Mixed) {
+            MixedQR<N> qm;
+            jacobian_pass_mixed(x, fnorm, st, qm, finite);
+            if (!finite) {
+                info = {NONFINITE, fnorm, 0.0, 0, false, false, false};
+                return;
+            }
+            if (qm.fits) {
+                trials(qm, st, x, info, fnorm, mu, mu_min_eff, false);
+                return;
+            }
+        }
+        StackedQR<N> q;
+        jacobian_pass<true>(x, fnorm, st, q, finite);
+        if (!finite) {
+            info = {NONFINITE, fnorm, 0.0, 0, false, false, false};
+            return;
+        }
+        trials(q, st, x, info, fnorm, mu, mu_min_eff, Mixed);
     }
 
     // stationary_converged, src/nonlinear/solver.jl:148-158.

@@ -90,3 +90,39 @@ def test_lm_hostile_and_exact(gsb, oracle):
     assert np.array_equal(sg["code"][:4], so["code"][:4])
     assert np.array_equal(sg["iterations"][:4], so["iterations"][:4])
     assert sg["code"][0] == so["code"][0] and sg["code"][1] == so["code"][1]
+
+
+@pytest.mark.gpu
+def test_lm_fp32_factor_with_refinement(gsb, oracle):
+    """The mixed form of the fit (FP32 stacked Givens factor, FP64 Gram matrix, gradient and
+    refinement) against the FP64 oracle. Its FP32 steps move the path of this ill-conditioned
+    fit further than the oracle's own one-ulp envelope: codes agree on at least 98 % of the
+    systems, and where both converge the objective agrees to 1e-10 on at least 98 % of them
+    (to 1e-6 on all)."""
+    import torch
+
+    X0, Y, t = c2(16384)
+    prob = gsb.LeastSquaresProblem(gsb.ExpSum3(t))
+    m = gsb.Newton(linsolve=gsb.QRFactorization("float32"), globalization=gsb.LevenbergMarquardt())
+    opts = gsb.Options(f_abstol=1e-12, f_reltol=0.0, max_iterations=50)
+    X = torch.tensor(X0, device="cuda")
+    S = gsb.status_buffer(X0.shape[0])
+    gsb.solve_batch(X, S, prob, m, gsb.PerSystem(torch.tensor(Y, device="cuda")), options=opts)
+    sg = gsb.statuses(S)
+    m64 = gsb.Newton(linsolve=gsb.QRFactorization(), globalization=gsb.LevenbergMarquardt())
+    _, so = oracle.solve_batch(prob, m64, X0.copy(), Y, opts)
+    assert np.mean(sg["code"] != so["code"]) <= 0.02
+    conv = (sg["code"] == 0) & (so["code"] == 0)
+    assert np.mean(conv) >= 0.45
+    fr = np.abs(sg["fnorm"] - so["fnorm"]) / so["fnorm"]
+    # the stationarity test stops within g_tol of the minimiser, and the FP32 steps reach it
+    # from elsewhere: a few converged systems stop at a slightly different objective
+    assert np.mean(fr[conv] <= F_TOL) >= 0.98, np.mean(fr[conv] <= F_TOL)
+    assert np.all(fr[conv] <= 1e-6), fr[conv].max()
+    assert not sg["promoted"].any()  # every row of this data fits FP32
+
+
+def test_lm_refinement_is_refused(gsb):
+    with pytest.raises(gsb.ArgumentError):
+        gsb.Newton(linsolve=gsb.QRFactorization(), globalization=gsb.LevenbergMarquardt(),
+                   refinement=gsb.Refinement())

@@ -41,7 +41,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="gsb200", choices=["gsb200", "reference"])
     ap.add_argument("--nsys", type=int, default=NSYS)
-    ap.add_argument("--profile", choices=["plain", "mixed", "lm", "irk", "mlp"], default=None,
+    ap.add_argument("--profile", choices=["plain", "mixed", "lm", "irk", "mlp", "shared"],
+                    default=None,
                     help="run `--warmup` + `--steps` solves of one form only (for ncu captures): "
                          "the cubic-affine batch of size --n, or the exponential-sum fit (lm)")
     ap.add_argument("--workload", choices=["c1", "c0", "c2", "c3", "c4"], default="c1",
@@ -505,17 +506,26 @@ def run_profile(args):
                      else cubic_affine(n, args.nsys, n + 1.0, 4))
         prob = G.NonlinearProblem(G.CubicAffine(n))
         plain, mixed = methods(G)
-        m = plain if args.profile == "plain" else mixed
+        m = mixed if args.profile == "mixed" else plain
     X0 = torch.tensor(X0_h, device="cuda")
     P = G.PerSystem(torch.tensor(P_h, device="cuda"))
+    if args.profile == "shared":
+        # BatchParams: the first system's A shared by the batch, every system's own b
+        n = X0_h.shape[1]
+        A = torch.tensor(P_h[0, :n * n].reshape(n, n).T.copy(), device="cuda")
+        P = G.BatchParams(A, torch.tensor(P_h[:, n * n:].copy(), device="cuda"))
     X = torch.empty_like(X0)
     S = G.status_buffer(args.nsys)
-    for _ in range(args.warmup + args.steps):
+    stream = torch.cuda.current_stream()
+
+    def step():
         X.copy_(X0)
         G.solve_batch(X, S, prob, m, P, options=options(G))
-    torch.cuda.synchronize()
+
+    ms = _events_ms(step, args.steps, args.warmup, stream)
     st = G.statuses(S)
-    print(json.dumps({"profile": args.profile, "nsys": args.nsys,
+    print(json.dumps({"profile": args.profile, "nsys": args.nsys, "ms_per_step": ms,
+                      "systems_per_s": args.nsys / (ms * 1e-3),
                       "codes": np.bincount(st["code"], minlength=6).tolist()}))
 
 

@@ -9,6 +9,7 @@ from .abi import ReturnCode, SOLVER_STATUS_DTYPE, load_library
 from .api import (
     ArgumentError,
     Backtracking,
+    BatchParams,
     BatchSummary,
     CubicAffine,
     Coupled2,

@@ -458,6 +458,17 @@ class PerSystem:
         self.data = data
 
 
+class BatchParams:
+    """BatchParams(shared, per_system), src/nonlinear/batched.jl:34-47: system i receives
+    (shared, per_system[i]). For CubicAffine, `shared` is the batch's n×n matrix A (a float64
+    tensor on the device of X, or anything numpy takes) and `per_system` the right-hand sides b,
+    an (nsys, n) tensor or SoA of an (n, nsys) tensor."""
+
+    def __init__(self, shared, per_system):
+        self.shared = shared
+        self.per_system = per_system
+
+
 class ReturnCodeCounts(NamedTuple):
     SUCCESS: int
     STALLED: int

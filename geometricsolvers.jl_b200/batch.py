@@ -12,9 +12,12 @@ from __future__ import annotations
 
 import ctypes
 
+import numpy as np
+
 from . import abi
 from .api import (
     ArgumentError,
+    BatchParams,
     BatchSummary,
     DimensionMismatch,
     NonlinearProblem,
@@ -69,6 +72,24 @@ def _is_perm(order, n):
     return bool(seen.all())
 
 
+def _shared_matrix(fam, A, device):
+    """The shared matrix of a CubicAffine BatchParams, column-major, as a float64 tensor on the
+    device of the batch."""
+    import torch
+
+    if fam.family != abi.Family.CUBIC_AFFINE:
+        raise ArgumentError("BatchParams takes a CubicAffine family (a shared A, per-system b)")
+    if isinstance(A, torch.Tensor):
+        if A.device != device:
+            raise ArgumentError("the shared matrix must be on the device of X")
+        At = A.to(torch.float64)
+    else:
+        At = torch.as_tensor(np.asarray(A, dtype=np.float64), device=device)
+    if tuple(At.shape) != (fam.n, fam.n):
+        raise DimensionMismatch(f"the shared matrix must be ({fam.n}, {fam.n}), got {tuple(At.shape)}")
+    return At.t().contiguous().reshape(-1)  # column-major: A[i, k] at i + k n
+
+
 def solve_batch(X, S, prob=None, method=None, p=None, *, order=None, options=None, stream=None,
                 **kwargs):
     """Solve every system of X in place (see the module docstring). X is an (nsys, n) float64
@@ -94,13 +115,17 @@ def solve_batch(X, S, prob=None, method=None, p=None, *, order=None, options=Non
         if Xt.dim() != 2 or Xt.shape[0] != fam.n:
             raise DimensionMismatch(f"SoA X must be ({fam.n}, nsys), got {tuple(Xt.shape)}")
         nsys = Xt.shape[1]
-    # parameters: PerSystem only (the families take per-system data)
+    # parameters: PerSystem blocks, or BatchParams (a shared A and per-system b) for CubicAffine
+    shared_A = None
+    if isinstance(p, BatchParams):
+        shared_A = _shared_matrix(fam, p.shared, Xt.device)
+        p = PerSystem(p.per_system)
     if not isinstance(p, PerSystem):
-        raise ArgumentError("p must be a PerSystem of per-system parameter blocks")
+        raise ArgumentError("p must be a PerSystem of per-system parameter blocks or a BatchParams")
     Pt = _tensor(p.data)
     p_layout = abi.GSB_SOA if isinstance(p.data, SoA) else abi.GSB_AOS
     _check_device_f64(Pt, "PerSystem data")
-    npar = fam.param_count
+    npar = fam.n if shared_A is not None else fam.param_count
     plen = Pt.shape[0] if p_layout == abi.GSB_AOS else (Pt.shape[1] if Pt.dim() == 2 else -1)
     if Pt.dim() != 2 or plen != nsys:
         raise DimensionMismatch(
@@ -138,6 +163,8 @@ def solve_batch(X, S, prob=None, method=None, p=None, *, order=None, options=Non
     lib = abi.load_library()
     sh = prob.shared_device(Xt.device)
     gp = prob.to_abi(None if sh is None else sh.data_ptr())
+    if shared_A is not None:
+        gp.shared, gp.shared_len = shared_A.data_ptr(), shared_A.numel()
     go = opt.to_abi()
     if stream is None:
         stream = torch.cuda.current_stream(Xt.device)
@@ -290,16 +317,23 @@ def solve_batch_host(X, S, prob, method, p, *, chunk=0, options=None, device=Non
     if X.dim() != 2 or X.shape[1] != fam.n:
         raise DimensionMismatch(f"X must be (nsys, {fam.n}), got {tuple(X.shape)}")
     nsys = X.shape[0]
+    device = torch.device(device or "cuda")
+    shared_A = None
+    if isinstance(p, BatchParams):  # the shared A goes to the device once, b streams per chunk
+        A = p.shared.cpu() if isinstance(p.shared, torch.Tensor) else p.shared
+        shared_A = _shared_matrix(fam, A, torch.device("cpu")).to(device)
+        p = PerSystem(p.per_system)
     if not isinstance(p, PerSystem):
-        raise ArgumentError("p must be a PerSystem of per-system parameter blocks")
+        raise ArgumentError("p must be a PerSystem of per-system parameter blocks or a BatchParams")
     Pt = p.data
     if not (isinstance(Pt, torch.Tensor) and Pt.device.type == "cpu" and Pt.dtype == torch.float64
             and Pt.is_contiguous() and Pt.dim() == 2):
         raise ArgumentError("PerSystem data must be a contiguous (nsys, np) float64 host tensor")
     if Pt.shape[0] != nsys:
         raise DimensionMismatch(f"PerSystem parameter length {Pt.shape[0]} does not match batch length {nsys}")
-    if Pt.shape[1] != fam.param_count:
-        raise DimensionMismatch(f"each system takes {fam.param_count} parameters")
+    npar = fam.n if shared_A is not None else fam.param_count
+    if Pt.shape[1] != npar:
+        raise DimensionMismatch(f"each system takes {npar} parameters")
     opt = _resolve_options(options, kwargs)
     counts_form = S is None
     if counts_form:
@@ -314,10 +348,11 @@ def solve_batch_host(X, S, prob, method, p, *, chunk=0, options=None, device=Non
     gm, go = method.to_abi(), opt.to_abi()
     if nsys == 0:
         return ReturnCodeCounts(0, 0, 0, 0, 0, 0) if counts_form else S
-    device = torch.device(device or "cuda")
     lib = abi.load_library()
     sh = prob.shared_device(device)
     gp = prob.to_abi(None if sh is None else sh.data_ptr())
+    if shared_A is not None:
+        gp.shared, gp.shared_len = shared_A.data_ptr(), shared_A.numel()
     tally = abi.GsbTally()
     with torch.cuda.device(device):
         _raise_for(lib.gsb_solve_batch_host(

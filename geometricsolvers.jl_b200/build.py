@@ -1,7 +1,8 @@
 """Builds libgsb.so (the CUDA kernels and the C-ABI) in this directory, for sm_100a.
 
 Each csrc/*.cu is compiled to an object in parallel (the kernel instantiations are spread over
-several translation units), then the objects are linked into one shared library.
+several translation units), then the objects are linked into one shared library. An object newer
+than its source and every header is reused.
 
 python geometricsolvers.jl_b200/build.py [--verbose]
 """
@@ -45,9 +46,19 @@ def up_to_date() -> bool:
     return all(os.path.getmtime(f) <= t for f in files)
 
 
-def _compile(src: str, verbose: bool):
+def _fresh(src: str, obj: str) -> bool:
+    """An object is kept when it is newer than its source and every header."""
+    if not os.path.exists(obj):
+        return False
+    t = os.path.getmtime(obj)
+    return all(os.path.getmtime(f) <= t for f in [os.path.join(CSRC, src), *_headers()])
+
+
+def _compile(src: str, verbose: bool, force: bool = True):
     nvcc = os.environ.get("NVCC", "nvcc")
     obj = os.path.join(OBJ, src[:-3] + ".o")
+    if not force and not verbose and _fresh(src, obj):
+        return src, obj, subprocess.CompletedProcess([], 0, "", "")
     cmd = [nvcc, *NVCC_FLAGS, "-c", os.path.join(CSRC, src), "-o", obj]
     if verbose:
         cmd += ["-Xptxas", "-v"]
@@ -76,7 +87,7 @@ def build(verbose: bool = False, force: bool = False, jobs: int = 0) -> str:
     os.makedirs(OBJ, exist_ok=True)
     jobs = jobs or max(1, min(len(sources()), os.cpu_count() or 1))
     with ThreadPoolExecutor(jobs) as pool:
-        results = list(pool.map(lambda s: _compile(s, verbose), sources()))
+        results = list(pool.map(lambda s: _compile(s, verbose, force), sources()))
     failed = [r for r in results if r[2].returncode != 0]
     for src, _, proc in results:
         if verbose or proc.returncode != 0:

@@ -19,17 +19,26 @@ namespace gsb {
 // Dual rules: the product of duals a*b has partials a.p b.v + b.p a.v, so with the seed
 // e_i the partial of (x_i x_i) x_i is (x_i + x_i) x_i + x_i x_i, and
 // J_ii = fma(0.1, that, A_ii).
-template <int N_> struct CubicAffine {
-    static constexpr int N = N_, M = N_, NP = N_ * N_ + N_;
+template <int N_, bool SharedA = false> struct CubicAffineT {
+    static constexpr int N = N_, M = N_;
+    // Parameters of a system: (A, b), or with SharedA (BatchParams, src/nonlinear/batched.jl:
+    // 34-47) only b, A being the batch's shared block.
+    static constexpr int NP = SharedA ? N_ : N_ * N_ + N_;
+    static constexpr int kShared = SharedA ? N_ * N_ : 0;  // doubles of the CTA-shared block
     static constexpr bool lsq = false;
-    const double* p;  // this system's parameter block in shared memory, entry k at p[k]
+    const double* p;            // this system's parameter block in shared memory
+    const double* a = nullptr;  // the shared A (column-major) in shared memory, with SharedA
     struct JState {
         double diag[N];
     };
     // The block stays in shared memory and is read at each use (a volatile shared load), rather
     // than hoisted out of the Newton loop into registers, which the factor needs.
     __device__ __forceinline__ double par(int k) const { return lds(smem_addr(p) + 8u * k); }
-    __device__ __forceinline__ double A(int i, int k) const { return par(i + k * N); }
+    __device__ __forceinline__ double A(int i, int k) const {
+        if constexpr (SharedA) return lds(smem_addr(a) + 8u * (i + k * N));
+        return par(i + k * N);
+    }
+    __device__ __forceinline__ double bv(int i) const { return SharedA ? par(i) : par(N * N + i); }
     __device__ __forceinline__ void F(const double (&x)[N], double (&out)[M]) const {
 #pragma unroll
         for (int i = 0; i < N; ++i) {
@@ -37,7 +46,7 @@ template <int N_> struct CubicAffine {
 #pragma unroll
             for (int j = 1; j < N; ++j) t = __fma_rn(A(i, j), x[j], t);
             double c = __dmul_rn(__dmul_rn(x[i], x[i]), x[i]);
-            out[i] = __dsub_rn(__fma_rn(0.1, c, t), par(N * N + i));
+            out[i] = __dsub_rn(__fma_rn(0.1, c, t), bv(i));
         }
     }
     __device__ __forceinline__ void jacobian(const double (&x)[N], JState& js) const {
@@ -64,6 +73,16 @@ template <int N_> struct CubicAffine {
             out[i] = __fma_rn(0.1, cp, t);
         }
     }
+};
+template <int N> using CubicAffine = CubicAffineT<N, false>;
+template <int N> using CubicAffineSharedA = CubicAffineT<N, true>;
+
+// The shared block of a family (0 doubles for families without one).
+template <class Fam, class = void> struct SharedLen {
+    static constexpr int value = 0;
+};
+template <class Fam> struct SharedLen<Fam, decltype(void(Fam::kShared))> {
+    static constexpr int value = Fam::kShared;
 };
 
 // A family with an analytic Jacobian (the problem's `J`, src/ad/forwarddiff_static.jl:36-38)

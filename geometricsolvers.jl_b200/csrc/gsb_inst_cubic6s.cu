@@ -1,0 +1,7 @@
+// Kernels of the BatchParams form of CubicAffine<6>: the matrix A shared by the batch (staged
+// once per CTA), the right-hand side b per system.
+#include "gsb_kernel_impl.cuh"
+
+namespace gsb {
+GSB_DEFINE_ENTRY(cubic6s, CubicAffineSharedA<6>)
+}  // namespace gsb

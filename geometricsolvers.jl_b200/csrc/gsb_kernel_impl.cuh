@@ -162,12 +162,18 @@ __global__ void __launch_bounds__(kThreads, (min_blocks<Fam, Mixed>())) newton_k
                                  const __grid_constant__ Launch L) {
     extern __shared__ double smem[];
     constexpr int N = Fam::N, NP = Fam::NP, RS = row_stride(NP, N);
+    // a family's block shared by the batch (BatchParams) first, then one row per thread
+    constexpr int SH = SharedLen<Fam>::value, SHP = ((SH + 1) / 2) * 2;
     const int tid = threadIdx.x;
-    double* prow = smem + tid * RS;
+    double* rows = smem + SHP;
+    double* prow = rows + tid * RS;
+    if constexpr (SH > 0) {
+        for (int q = tid; q < SH; q += kThreads) smem[q] = __ldg(L.shared + q);
+    }
     for_each_chunk<Persistent>(L, kThreads, [&](int64_t base, const Range& r) {
         const int64_t i = base + tid;
         if (r.order == nullptr && L.p_layout == GSB_AOS && L.p_off == nullptr) {
-            stage_aos<NP, RS, kThreads>(smem, L.P + base * NP, r.n - base, tid);
+            stage_aos<NP, RS, kThreads>(rows, L.P + base * NP, r.n - base, tid);
         } else if (i < r.n) {
             const int64_t idx = r.order ? r.order[i] - L.order_base : i;
             if (L.p_layout == GSB_SOA) {
@@ -183,6 +189,7 @@ __global__ void __launch_bounds__(kThreads, (min_blocks<Fam, Mixed>())) newton_k
         if (i >= r.n) return;
         const int64_t idx = r.order ? r.order[i] - L.order_base : i;
         Fam fam{prow};
+        if constexpr (SH > 0) fam.a = smem;
         double x[N];
         double* xb = x_block(L, idx, N);
 #pragma unroll
@@ -368,7 +375,8 @@ struct KernelEntry {
 template <class Fam, bool F, bool Mixed, bool PlainRef> KernelEntry* entry() {
     static KernelEntry e{newton_kernel<Fam, F, Mixed, PlainRef, false>,
                          newton_kernel<Fam, F, Mixed, PlainRef, true>,
-                         kThreads * row_stride(Fam::NP, Fam::N), kThreads, {}};
+                         ((SharedLen<Fam>::value + 1) / 2) * 2 + kThreads * row_stride(Fam::NP, Fam::N),
+                         kThreads, {}};
     return &e;
 }
 

@@ -150,10 +150,17 @@ int workspace(Workspace** out) {
     return 0;
 }
 
+// The cubic family's BatchParams form: the batch's matrix A in prob->shared (n^2 doubles).
+bool shared_matrix(const GsbProblem* p) {
+    return p->family == GSB_FAMILY_CUBIC_AFFINE && p->shared && p->shared_len == (int64_t)p->n * p->n;
+}
+
 int64_t param_count(const GsbProblem* p) {
     switch (p->family) {
     case GSB_FAMILY_CUBIC_AFFINE:
-        return (p->n >= 1 && p->n <= 32) ? (int64_t)p->n * p->n + p->n : GSB_ERR_ARGUMENT;
+        if (!(p->n >= 1 && p->n <= 32)) return GSB_ERR_ARGUMENT;
+        // with A shared by the batch (shared_len = n^2), a system's block is b alone
+        return shared_matrix(p) ? (int64_t)p->n : (int64_t)p->n * p->n + p->n;
     case GSB_FAMILY_EXPSUM3_LSQ: return p->m;
     case GSB_FAMILY_IRK3_HENON_HEILES: return 4;
     case GSB_FAMILY_HETERO6: return 1;
@@ -170,6 +177,11 @@ GSB_DECLARE_ENTRY(cubic3);
 GSB_DECLARE_ENTRY(cubic4);
 GSB_DECLARE_ENTRY(cubic6);
 GSB_DECLARE_ENTRY(cubic8);
+GSB_DECLARE_ENTRY(cubic2s);
+GSB_DECLARE_ENTRY(cubic3s);
+GSB_DECLARE_ENTRY(cubic4s);
+GSB_DECLARE_ENTRY(cubic6s);
+GSB_DECLARE_ENTRY(cubic8s);
 GSB_DECLARE_ENTRY(hetero6);
 GSB_DECLARE_ENTRY(coupled2);
 GSB_DECLARE_TEAM(cubic6);
@@ -196,6 +208,19 @@ int tuned_team(const GsbProblem* prob, bool mixed) {
 
 // The kernel of a call: the one-thread solve for T = 1, else the team solve (fused only).
 KernelEntry* select_kernel(const GsbProblem* prob, bool fused, bool mixed, bool refine, int T) {
+    if (shared_matrix(prob)) {
+        // BatchParams: A shared by the batch and staged once per CTA, b per system; one thread
+        // per system (the warp and team forms read a whole (A, b) block per system)
+        if (T > 1) return nullptr;
+        switch (prob->n) {
+        case 2: return entry_cubic2s(fused, mixed, refine);
+        case 3: return entry_cubic3s(fused, mixed, refine);
+        case 4: return entry_cubic4s(fused, mixed, refine);
+        case 6: return entry_cubic6s(fused, mixed, refine);
+        case 8: return entry_cubic8s(fused, mixed, refine);
+        default: return nullptr;
+        }
+    }
     if (prob->family == GSB_FAMILY_CUBIC_AFFINE && prob->n >= 12) {
         // the warp form: 16 lanes per system up to n = 16 (or a whole warp), a whole warp above
         if (T == 0) T = prob->n <= 16 ? 16 : 32;

@@ -60,6 +60,32 @@ def test_param_counts(gsb):
         assert lib.gsb_param_count(ctypes.byref(p)) == expect == fam.param_count
 
 
+def test_batch_params_form(gsb):
+    # BatchParams of the cubic family (src/nonlinear/batched.jl:34-47): with the shared A in
+    # `shared` (n^2 doubles) a system's block is b alone; other shared lengths keep (A, b)
+    import numpy as np
+    import torch
+
+    _shared_matrix = gsb.batch._shared_matrix
+    lib = gsb.load_library()
+    A = torch.arange(64, dtype=torch.float64).reshape(8, 8)
+    p = gsb.NonlinearProblem(gsb.CubicAffine(8)).to_abi()
+    p.shared, p.shared_len = A.data_ptr(), 64
+    assert lib.gsb_param_count(ctypes.byref(p)) == 8
+    p.shared_len = 63
+    assert lib.gsb_param_count(ctypes.byref(p)) == 72
+    col = _shared_matrix(gsb.CubicAffine(8), A, torch.device("cpu"))
+    assert np.array_equal(col.numpy(), A.numpy().flatten(order="F"))
+    with pytest.raises(gsb.DimensionMismatch):
+        _shared_matrix(gsb.CubicAffine(8), A[:4], torch.device("cpu"))
+    with pytest.raises(gsb.ArgumentError):
+        _shared_matrix(gsb.Coupled2(), A, torch.device("cpu"))
+    with pytest.raises(gsb.ArgumentError):
+        gsb.solve_batch_host(torch.zeros(4, 2, dtype=torch.float64), None,
+                             gsb.NonlinearProblem(gsb.Coupled2()), gsb.Newton(),
+                             gsb.BatchParams(A, torch.zeros(4, 2, dtype=torch.float64)))
+
+
 def test_host_checks_refuse_before_any_launch(gsb):
     # constructor checks of the reference (src/base/options.jl:207-236, backtracking.jl:34-40,
     # newton.jl:160-176); a host tensor is refused (the solver has no host path)

@@ -77,10 +77,12 @@ __device__ __forceinline__ void cswap(int r, int p, float& x, float& y) {
 // factor_matrix (src/linear/factors.jl:802-811): TF = T divides by 2^e only for e < 0; another
 // TF divides for every e != 0, in T, then rounds to TF.
 template <bool F, int N, class TF> struct LUFactor {
-    // Under fused arithmetic the Float32 factor of the mixed step (whose result the Float64
-    // refinement corrects) divides by multiplying with reciprocals: of each pivot, and of the
-    // scale s of its right-hand sides.
-    static constexpr bool kRecip = F && sizeof(TF) == sizeof(float);
+    // Under fused arithmetic the factor divides by multiplying with reciprocals: one of each
+    // pivot, computed once and kept in place of the pivot for the back substitution (8 FP64
+    // divisions instead of 36 at n = 8, where one division costs the FP64 pipe about 14 FMAs),
+    // and, for the Float32 factor of the mixed step, one of the scale s of its right-hand sides.
+    // The unfused arithmetic divides as lu.jl does.
+    static constexpr bool kRecip = F;
     TF a[N * N];
     int ipiv[N];
     int info;
@@ -284,6 +286,16 @@ template <bool F, int N> struct LocalLU {
             double akk = a[k + k * N];
             if (akk == 0.0) {
                 if (info == 0) info = k + 1;
+            } else if constexpr (F) {
+                const double r = 1.0 / akk;
+                a[k + k * N] = r;
+#pragma unroll 1
+                for (int i = k + 1; i < N; ++i) a[i + k * N] = a[i + k * N] * r;
+#pragma unroll 1
+                for (int j = k + 1; j < N; ++j)
+#pragma unroll 1
+                    for (int i = k + 1; i < N; ++i)
+                        a[i + j * N] = Arith<F>::msub(a[i + k * N], a[k + j * N], a[i + j * N]);
             } else {
 #pragma unroll 1
                 for (int i = k + 1; i < N; ++i) a[i + k * N] = a[i + k * N] / akk;
@@ -314,7 +326,7 @@ template <bool F, int N> struct LocalLU {
         }
 #pragma unroll 1
         for (int k = N - 1; k >= 0; --k) {
-            double xk = x[k] / a[k + k * N];
+            double xk = F ? x[k] * a[k + k * N] : x[k] / a[k + k * N];
             x[k] = xk;
 #pragma unroll 1
             for (int i = 0; i < k; ++i) x[i] = Arith<F>::msub(a[i + k * N], xk, x[i]);

@@ -265,8 +265,9 @@ template <int N, int T, bool F> struct WarpVec {
 // pivot of column k in `piv`.
 template <int N, int T, bool F, class TF> struct WarpLU {
     static constexpr int LD = warp_ld(N);
-    // the fused Float32 factor divides by multiplying with reciprocals (see LUFactor)
-    static constexpr bool kRecip = F && sizeof(TF) == sizeof(float);
+    // the fused factor divides by multiplying with pivot reciprocals (see LUFactor); in the
+    // back substitution that takes a division off each of the N sequential steps
+    static constexpr bool kRecip = F;
     using A = Arith<F>;
     TF* a;
     int piv;

@@ -134,7 +134,8 @@ typedef enum { GSB_LU = 0, GSB_QR = 1 } GsbLinsolve;
 typedef enum { GSB_F64 = 0, GSB_F32 = 1 } GsbPrecision;
 typedef enum { GSB_NO_REFINEMENT = 0, GSB_REFINEMENT = 1 } GsbRefinementKind;
 /* The rounding of the linear algebra (factorisation, solves, norms, products with the Jacobian).
- * GSB_FUSED contracts each product-and-sum into one fused multiply-add (the fast default);
+ * GSB_FUSED contracts each product-and-sum into one fused multiply-add and divides by a pivot
+ * through its reciprocal (the fast default; results agree with the reference to rounding);
  * GSB_UNFUSED rounds every product and every sum on its own, as Julia evaluates `a * b + c`, so
  * that a batch reproduces a CPU restatement of the reference bit for bit. Residual families fix
  * their own operation order and are the same under both. */

@@ -202,18 +202,28 @@ template <int L, class T> __device__ __forceinline__ T rmaxnorm(const T (&a)[L])
     return m;
 }
 
-// matrix_exponent over the bits of |a| (src/linear/factors.jl:833-843).
+// matrix_exponent over the bits of |a| (src/linear/factors.jl:833-843): the exponent of the
+// largest |a_i| (0 when it is zero or not finite), clamped to [-1023, 1023]. The largest |a_i|
+// has the largest high word (sign shifted out), so a tree of 32-bit maxima (associative: the
+// order does not matter) gives its exponent field: for a normal maximum the field is the
+// exponent; a subnormal maximum has an exponent below -1022, which the clamp makes -1023; Inf
+// and NaN give 0; and when every high word is zero the low words tell zero from subnormal.
 template <int L> __device__ __forceinline__ int matrix_exponent(const double (&a)[L]) {
-    unsigned long long mb = 0;
+    unsigned h[L];
 #pragma unroll
-    for (int i = 0; i < L; ++i) {
-        unsigned long long b = FBits<double>::bits(a[i]) & ~FBits<double>::sign_mask;
-        mb = b > mb ? b : mb;
-    }
-    double m = FBits<double>::from(mb);
-    if (!(isfin(m) && m != 0.0)) return 0;
-    int e = jexponent(m);
-    return e > 1023 ? 1023 : (e < -1023 ? -1023 : e);
+    for (int i = 0; i < L; ++i) h[i] = (unsigned)__double2hiint(a[i]) << 1;
+#pragma unroll
+    for (int w = 1; w < L; w *= 2)
+#pragma unroll
+        for (int i = 0; i + w < L; i += 2 * w) h[i] = h[i] > h[i + w] ? h[i] : h[i + w];
+    const int field = (int)(h[0] >> 21);
+    if (field == 2047) return 0;          // Inf or NaN
+    if (field != 0) return field - 1023;  // normal: in [-1022, 1023]
+    if (h[0] != 0) return -1023;          // subnormal
+    unsigned lo = 0;
+#pragma unroll
+    for (int i = 0; i < L; ++i) lo |= (unsigned)__double2loint(a[i]);
+    return lo != 0 ? -1023 : 0;           // subnormal, or all zero
 }
 
 // headroom(n) = 2 + ceil(log2 n) (src/linear/factors.jl:890), a constant of the size.

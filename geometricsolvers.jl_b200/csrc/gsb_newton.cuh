@@ -88,6 +88,38 @@ template <bool F, int N, class TF> struct LUFactor {
     int info;
     int e;
 
+    // J into the Float64 factor's registers, with the two sums that grad_ratio_and_norm takes
+    // over J folded while each entry is in a register: s, the squares of the entries in column
+    // order, and g = J' Fx, each in the order of that function's own loops, so the results are
+    // the same bits and J is read from the family once per step instead of three times.
+    template <class Fam, class JS, int M>
+    __device__ __forceinline__ void load(const Fam& fam, const JS& js, const double (&Fx)[M],
+                                         double& s, double (&g)[N]) {
+        static_assert(sizeof(TF) == sizeof(double) && M == N, "the square Float64 factor");
+#pragma unroll
+        for (int k = 0; k < N; ++k)
+#pragma unroll
+            for (int i = 0; i < N; ++i) {
+                const double v = fam.J(js, i, k);
+                a[i + k * N] = v;
+                s = (i == 0 && k == 0) ? Arith<F>::mul(v, v) : Arith<F>::madd(v, v, s);
+                g[k] = i == 0 ? Arith<F>::mul(v, Fx[0]) : Arith<F>::madd(v, Fx[i], g[k]);
+            }
+    }
+
+    // factor_matrix's scaling of the loaded J (J / 2^e in place), then the elimination.
+    __device__ __forceinline__ void eliminate() {
+        static_assert(sizeof(TF) == sizeof(double), "the Float64 factor");
+        e = matrix_exponent<N * N>(a);
+        if (e < 0) {
+#pragma unroll
+            for (int q = 0; q < N * N; ++q) a[q] = scale2_in(a[q], -e);  // -e in [1, 1023]
+        } else {
+            e = 0;
+        }
+        elimination();
+    }
+
     template <class Fam, class JS>
     __device__ __forceinline__ void factor(const Fam& fam, const JS& js) {
         // J into the factor's registers, then J / 2^e in place (factor_matrix)
@@ -97,13 +129,8 @@ template <bool F, int N, class TF> struct LUFactor {
             for (int k = 0; k < N; ++k)
 #pragma unroll
                 for (int i = 0; i < N; ++i) a[i + k * N] = fam.J(js, i, k);
-            e = matrix_exponent<N * N>(a);
-            if (e < 0) {
-#pragma unroll
-                for (int q = 0; q < N * N; ++q) a[q] = scale2_in(a[q], -e);  // -e in [1, 1023]
-            } else {
-                e = 0;
-            }
+            eliminate();
+            return;
         } else {
             unsigned long long mb = 0;
 #pragma unroll
@@ -123,6 +150,11 @@ template <bool F, int N, class TF> struct LUFactor {
                     a[i + k * N] = TF(e == 0 ? v : scale2_in(v, -e));  // -e in [-1023, 1023]
                 }
         }
+        elimination();
+    }
+
+    // The pivoted elimination of the scaled matrix (lu.jl:24-64).
+    __device__ __forceinline__ void elimination() {
         info = 0;
 #pragma unroll
         for (int k = 0; k < N; ++k) {
@@ -376,6 +408,12 @@ template <class Fam, bool F, bool Mixed, bool PlainRef = false> struct Solver {
 #pragma unroll
         for (int i = 0; i < N; ++i) sts(a + 8u * i, x[i]);
     }
+    __device__ __forceinline__ void park_F(const double (&Fx)[M]) const {
+        if (stash == nullptr) return;
+        const unsigned a = smem_addr(stash);
+#pragma unroll
+        for (int i = 0; i < M; ++i) sts(a + 8u * (N + i), Fx[i]);
+    }
     __device__ __forceinline__ void unpark_x(double (&x)[N]) const {
         if (stash == nullptr) return;
         const unsigned a = smem_addr(stash);
@@ -406,7 +444,6 @@ template <class Fam, bool F, bool Mixed, bool PlainRef = false> struct Solver {
     __device__ void grad_ratio_and_norm(const JS& js, const double (&Fx)[M], double fnorm,
                                         double& gr, double& jnorm) const {
         double s = A::mul(fam.J(js, 0, 0), fam.J(js, 0, 0));
-        double m0 = 0.0;
 #pragma unroll
         for (int k = 0; k < N; ++k)
 #pragma unroll
@@ -442,7 +479,6 @@ template <class Fam, bool F, bool Mixed, bool PlainRef = false> struct Solver {
                 jnorm = scale2_in(sqrt(acc), e);
             }
         }
-        (void)m0;
         if (jnorm == 0.0 || fnorm == 0.0) {
             gr = 0.0;
             return;
@@ -470,6 +506,20 @@ template <class Fam, bool F, bool Mixed, bool PlainRef = false> struct Solver {
             g[j] = t;
         }
         gr = __ddiv_rn(__ddiv_rn(rnorm<F, N>(g), jnorm), ldexp(fnorm, -e));
+    }
+
+    // grad_ratio_and_norm's common branch from the two sums that the factor's load folds (s,
+    // the squares of J's entries in column order; g = J' Fx), with both sums in the range where
+    // their norms are plain square roots. False (nothing written) when either is not: the
+    // function above then runs in full, with the same operations, after the solve.
+    __device__ __forceinline__ bool grad_ratio_fast(double s, const double (&g)[N], double fnorm,
+                                                    double& gr, double& jnorm) const {
+        if (!(isfin(s) && s >= double(M * N) * kFloatmin)) return false;
+        const double gs = norm2<F, N>(g);
+        if (!(isfin(gs) && gs >= double(N) * kFloatmin)) return false;
+        jnorm = sqrt(s);
+        gr = fnorm == 0.0 ? 0.0 : __ddiv_rn(__ddiv_rn(sqrt(gs), jnorm), fnorm);
+        return true;
     }
 
     // residual_norm, src/nonlinear/newton.jl:1274-1278.
@@ -667,16 +717,25 @@ template <class Fam, bool F, bool Mixed, bool PlainRef = false> struct Solver {
         JS js;
         fam.jacobian(x, js);
         double gr, jn;
-        grad_ratio_and_norm(js, Fx, fnorm, gr, jn);
         double merit = st.merit;
         constexpr bool ref = PlainRef;
         {
-            park(x, Fx);
             LUFactor<F, N, double> fac;
-            fac.factor(fam, js);
+            park_x(x);
+            // grad_ratio_and_norm from the sums that the factor's load folds; its scaled
+            // branches, for sums out of range, run in full once the factor is done with
+            bool gr_done;
+            {
+                double s, g[N];
+                fac.load(fam, js, Fx, s, g);
+                gr_done = grad_ratio_fast(s, g, fnorm, gr, jn);
+            }
+            park_F(Fx);
+            fac.eliminate();
             if (fac.info > 0) {
                 unpark_x(x);
                 unpark_F(Fx);
+                if (!gr_done) grad_ratio_and_norm(js, Fx, fnorm, gr, jn);
                 info = {SINGULAR, rnorm<F, M>(Fx), 0.0, 0, false, false, false};
             } else {
                 double d[N];
@@ -685,6 +744,7 @@ template <class Fam, bool F, bool Mixed, bool PlainRef = false> struct Solver {
 #pragma unroll
                 for (int i = 0; i < N; ++i) d[i] = -d[i];
                 if constexpr (ref) refine(d, fac, js, Fx);
+                if (!gr_done) grad_ratio_and_norm(js, Fx, fnorm, gr, jn);
                 unpark_x(x);
                 globalize(x, Fx, d, !ref, merit, info);
             }

@@ -156,7 +156,7 @@ template <class Fam, bool Mixed> constexpr int min_blocks() {
 #endif
 }
 
-template <class Fam, bool F, bool Mixed, bool PlainRef, bool Persistent>
+template <class Fam, bool F, bool Mixed, bool PlainRef, bool Persistent, bool Qr = false>
 __global__ void __launch_bounds__(kThreads, (min_blocks<Fam, Mixed>())) newton_kernel(const __grid_constant__ GsbMethod m,
                                  const __grid_constant__ GsbOptions o,
                                  const __grid_constant__ Launch L) {
@@ -195,7 +195,7 @@ __global__ void __launch_bounds__(kThreads, (min_blocks<Fam, Mixed>())) newton_k
 #pragma unroll
         for (int k = 0; k < N; ++k)
             x[k] = L.x_layout == GSB_SOA ? L.X[(int64_t)k * L.nsys + idx] : xb[k];
-        Solver<Fam, F, Mixed, PlainRef> sv(fam, m, o, N >= 6 ? prow + NP : nullptr);
+        Solver<Fam, F, Mixed, PlainRef, Qr> sv(fam, m, o, N >= 6 ? prow + NP : nullptr);
         double gr;
         DevStatus s = sv.solve(x, gr);
 #pragma unroll
@@ -380,6 +380,15 @@ template <class Fam, bool F, bool Mixed, bool PlainRef> KernelEntry* entry() {
     return &e;
 }
 
+// The plain step with the static QR factor (QRFactorization, Float64, no refinement).
+template <class Fam, bool F> KernelEntry* qr_entry() {
+    static KernelEntry e{newton_kernel<Fam, F, false, false, false, true>,
+                         newton_kernel<Fam, F, false, false, true, true>,
+                         ((SharedLen<Fam>::value + 1) / 2) * 2 + kThreads * row_stride(Fam::NP, Fam::N),
+                         kThreads, {}};
+    return &e;
+}
+
 template <class Fam, bool F, bool Mixed> KernelEntry* lm_entry() {
     constexpr int RS = (Fam::M % 2 == 1) ? Fam::M : Fam::M + 1;
     static KernelEntry e{lm_kernel<Fam, F, Mixed>, nullptr, kThreads * RS + Fam::M, kThreads, {}};
@@ -426,6 +435,11 @@ template <class Fam> KernelEntry* pick(bool fused, bool mixed, bool refine) {
 }
 
 #define GSB_DECLARE_ENTRY(NAME) KernelEntry* entry_##NAME(bool fused, bool mixed, bool refine)
+#define GSB_DECLARE_QR(NAME) KernelEntry* qr_##NAME(bool fused)
+#define GSB_DEFINE_QR(NAME, ...)                                                              \
+    KernelEntry* qr_##NAME(bool fused) {                                                      \
+        return fused ? qr_entry<__VA_ARGS__, true>() : qr_entry<__VA_ARGS__, false>();        \
+    }
 #define GSB_DECLARE_TEAM(NAME) KernelEntry* team_##NAME(int T, bool mixed)
 #define GSB_DEFINE_ENTRY(NAME, ...)                                          \
     KernelEntry* entry_##NAME(bool fused, bool mixed, bool refine) {         \

@@ -177,6 +177,13 @@ GSB_DECLARE_ENTRY(cubic3);
 GSB_DECLARE_ENTRY(cubic4);
 GSB_DECLARE_ENTRY(cubic6);
 GSB_DECLARE_ENTRY(cubic8);
+GSB_DECLARE_QR(cubic2);
+GSB_DECLARE_QR(cubic3);
+GSB_DECLARE_QR(cubic4);
+GSB_DECLARE_QR(cubic6);
+GSB_DECLARE_QR(cubic8);
+GSB_DECLARE_QR(hetero6);
+GSB_DECLARE_QR(coupled2);
 GSB_DECLARE_ENTRY(cubic2s);
 GSB_DECLARE_ENTRY(cubic3s);
 GSB_DECLARE_ENTRY(cubic4s);
@@ -204,6 +211,26 @@ int tuned_team(const GsbProblem* prob, bool mixed) {
     (void)prob;
     (void)mixed;
     return 1;
+}
+
+// The kernel of a QRFactorization call: the one-thread plain step with the static QR factor
+// (Float64, no refinement), for the square families with per-system parameter blocks.
+KernelEntry* select_qr_kernel(const GsbProblem* prob, bool fused, int T) {
+    if (T > 1 || shared_matrix(prob)) return nullptr;
+    switch (prob->family) {
+    case GSB_FAMILY_CUBIC_AFFINE:
+        switch (prob->n) {
+        case 2: return qr_cubic2(fused);
+        case 3: return qr_cubic3(fused);
+        case 4: return qr_cubic4(fused);
+        case 6: return qr_cubic6(fused);
+        case 8: return qr_cubic8(fused);
+        default: return nullptr;
+        }
+    case GSB_FAMILY_HETERO6: return qr_hetero6(fused);
+    case GSB_FAMILY_COUPLED2: return qr_coupled2(fused);
+    default: return nullptr;
+    }
 }
 
 // The kernel of a call: the one-thread solve for T = 1, else the team solve (fused only).
@@ -331,10 +358,10 @@ int noalloc_scratch(unsigned long long** out) {
 }
 
 // Pick the kernel for the call and launch it on `st` (arguments already checked).
-int launch_solve(const GsbProblem* prob, const GsbMethod* method, const GsbOptions* opt, double* X,
-                 int32_t x_layout, void* S, int32_t s_kind, const double* P, int32_t p_layout,
-                 const int64_t* order, int32_t order_base, int64_t nsys, cudaStream_t st,
-                 unsigned long long* tally_dev) {
+// The kernel of a call (family, size, method): the least-squares family's LevenbergMarquardt
+// kernel, the QRFactorization kernel, or the LU kernels of select_kernel. An error (and no
+// kernel) for a combination without one.
+int select_entry(const GsbProblem* prob, const GsbMethod* method, KernelEntry** out) {
     const bool mixed = method->factor_precision == GSB_F32;
     const bool fused = method->arithmetic == GSB_FUSED;
     const bool lm = method->globalization == GSB_LEVENBERG_MARQUARDT;
@@ -356,14 +383,30 @@ int launch_solve(const GsbProblem* prob, const GsbMethod* method, const GsbOptio
         if (lm)
             return set_err(GSB_ERR_UNSUPPORTED,
                            "LevenbergMarquardt batch kernel only for least-squares families");
-        if (method->linsolve != GSB_LU)
-            return set_err(GSB_ERR_UNSUPPORTED, "QRFactorization batch kernel not in this build");
-        if (prob->family == GSB_FAMILY_IRK3_HENON_HEILES && !prob->shared)
-            return set_err(GSB_ERR_ARGUMENT, "the step h and the tableau A are missing");
-        ke = select_kernel(prob, fused, mixed, method->refinement == GSB_REFINEMENT,
-                           method->threads_per_system);
+        if (method->linsolve == GSB_QR) {
+            if (mixed || method->refinement == GSB_REFINEMENT)
+                return set_err(GSB_ERR_UNSUPPORTED,
+                               "the QRFactorization batch kernel takes a Float64 factor and no "
+                               "refinement");
+            ke = select_qr_kernel(prob, fused, method->threads_per_system);
+        } else {
+            if (prob->family == GSB_FAMILY_IRK3_HENON_HEILES && !prob->shared)
+                return set_err(GSB_ERR_ARGUMENT, "the step h and the tableau A are missing");
+            ke = select_kernel(prob, fused, mixed, method->refinement == GSB_REFINEMENT,
+                               method->threads_per_system);
+        }
     }
     if (!ke) return set_err(GSB_ERR_UNSUPPORTED, "no batch kernel for this family and size");
+    *out = ke;
+    return 0;
+}
+
+int launch_solve(const GsbProblem* prob, const GsbMethod* method, const GsbOptions* opt, double* X,
+                 int32_t x_layout, void* S, int32_t s_kind, const double* P, int32_t p_layout,
+                 const int64_t* order, int32_t order_base, int64_t nsys, cudaStream_t st,
+                 unsigned long long* tally_dev) {
+    KernelEntry* ke = nullptr;
+    if (int rc = select_entry(prob, method, &ke)) return rc;
     int dev = 0;
     if (int rc = cuda_err(cudaGetDevice(&dev), "cudaGetDevice")) return rc;
     size_t smem = (size_t)ke->smem_doubles * sizeof(double);
@@ -481,35 +524,8 @@ int gsb_solve_batch(const GsbProblem* prob, const GsbMethod* method, const GsbOp
             seen[v] = 1;
         }
     }
-    const bool mixed = method->factor_precision == GSB_F32;
-    const bool fused = method->arithmetic == GSB_FUSED;
-    const bool lm = method->globalization == GSB_LEVENBERG_MARQUARDT;
     KernelEntry* ke = nullptr;
-    if (prob->family == GSB_FAMILY_EXPSUM3_LSQ) {
-        // the least-squares family: the LevenbergMarquardt step on its stacked QR path
-        if (!lm)
-            return set_err(GSB_ERR_UNSUPPORTED,
-                           "the least-squares batch kernel runs the LevenbergMarquardt step");
-        if (method->refinement == GSB_REFINEMENT)
-            return set_err(GSB_ERR_UNSUPPORTED,
-                           "Newton with a LevenbergMarquardt globalization takes no refinement");
-        if (method->threads_per_system > 1)
-            return set_err(GSB_ERR_UNSUPPORTED, "one thread per least-squares system");
-        if (prob->m != 64) return set_err(GSB_ERR_UNSUPPORTED, "no batch kernel for this m");
-        if (!prob->shared) return set_err(GSB_ERR_ARGUMENT, "the abscissae t are missing");
-        ke = lm_expsum3_64(fused, mixed);
-    } else {
-        if (lm)
-            return set_err(GSB_ERR_UNSUPPORTED,
-                           "LevenbergMarquardt batch kernel only for least-squares families");
-        if (method->linsolve != GSB_LU)
-            return set_err(GSB_ERR_UNSUPPORTED, "QRFactorization batch kernel not in this build");
-        if (prob->family == GSB_FAMILY_IRK3_HENON_HEILES && !prob->shared)
-            return set_err(GSB_ERR_ARGUMENT, "the step h and the tableau A are missing");
-        ke = select_kernel(prob, fused, mixed, method->refinement == GSB_REFINEMENT,
-                           method->threads_per_system);
-    }
-    if (!ke) return set_err(GSB_ERR_UNSUPPORTED, "no batch kernel for this family and size");
+    if (int rc = select_entry(prob, method, &ke)) return rc;
     Workspace* ws = nullptr;
     if (tally) {
         if (int rc = workspace(&ws)) return rc;

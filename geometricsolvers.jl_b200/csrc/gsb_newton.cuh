@@ -268,6 +268,124 @@ template <bool F, int N, class TF> struct LUFactor {
     }
 };
 
+// The static Householder QR of a square J without column pivoting (src/linear/static/qr.jl:
+// 9-60), one thread, the factor in registers: step k reflects the scaled subcolumn onto
+// -phase * sigma e_1 with tau_k = (sigma + |x_1|) / sigma in [1, 2] and the reflector's vector
+// w = v / v_1 stored below the diagonal; R on and above it. The same interface as LUFactor's
+// Float64 factor (load / eliminate / ldiv), so the plain step takes either. Divisions stay
+// divisions under both arithmetics; GSB_FUSED only contracts the products and sums.
+template <bool F, int N> struct QRFactor {
+    using A_ = Arith<F>;
+    double a[N * N];
+    double tau[N];
+    int info;
+    int e;
+
+    template <class Fam, class JS, int M>
+    __device__ __forceinline__ void load(const Fam& fam, const JS& js, const double (&Fx)[M],
+                                         double& s, double (&g)[N]) {
+        static_assert(M == N, "the square factor");
+#pragma unroll
+        for (int k = 0; k < N; ++k)
+#pragma unroll
+            for (int i = 0; i < N; ++i) {
+                const double v = fam.J(js, i, k);
+                a[i + k * N] = v;
+                s = (i == 0 && k == 0) ? A_::mul(v, v) : A_::madd(v, v, s);
+                g[k] = i == 0 ? A_::mul(v, Fx[0]) : A_::madd(v, Fx[i], g[k]);
+            }
+    }
+
+    template <class Fam, class JS> __device__ __forceinline__ void factor(const Fam& fam, const JS& js) {
+#pragma unroll
+        for (int k = 0; k < N; ++k)
+#pragma unroll
+            for (int i = 0; i < N; ++i) a[i + k * N] = fam.J(js, i, k);
+        eliminate();
+    }
+
+    // factor_matrix's scaling (J / 2^e), then the reflections (qr.jl:17-58).
+    __device__ __forceinline__ void eliminate() {
+        e = matrix_exponent<N * N>(a);
+        if (e < 0) {
+#pragma unroll
+            for (int q = 0; q < N * N; ++q) a[q] = scale2_in(a[q], -e);  // -e in [1, 1023]
+        } else {
+            e = 0;
+        }
+        info = 0;
+#pragma unroll
+        for (int k = 0; k < N; ++k) {
+            tau[k] = 0.0;
+            // the norm of the subcolumn as LAPACK's nrm2 takes it: divided by its largest |a|
+            double amax = 0.0;
+#pragma unroll
+            for (int i = k; i < N; ++i) amax = jmax(amax, fabs(a[i + k * N]));
+            double x[N];
+#pragma unroll
+            for (int i = 0; i < N; ++i)
+                x[i] = (i >= k && amax != 0.0) ? __ddiv_rn(a[i + k * N], amax) : 0.0;
+            const double sigma = __dmul_rn(amax, rnorm<F, N>(x));
+            if (sigma != 0.0) {
+                const double x1 = a[k + k * N];
+                const double ax1 = fabs(x1);
+                const double phase = x1 == 0.0 ? 1.0 : __ddiv_rn(x1, ax1);
+                const double sa = __dadd_rn(sigma, ax1);
+                const double v1 = __dmul_rn(phase, sa);
+                const double tk = __ddiv_rn(sa, sigma);
+                tau[k] = tk;
+#pragma unroll
+                for (int i = k + 1; i < N; ++i) a[i + k * N] = __ddiv_rn(a[i + k * N], v1);
+#pragma unroll
+                for (int j = k + 1; j < N; ++j) {
+                    double t = a[k + j * N];
+#pragma unroll
+                    for (int i = k + 1; i < N; ++i) t = A_::madd(a[i + k * N], a[i + j * N], t);
+                    t = __dmul_rn(t, tk);
+                    a[k + j * N] = __dsub_rn(a[k + j * N], t);
+#pragma unroll
+                    for (int i = k + 1; i < N; ++i) a[i + j * N] = A_::msub(a[i + k * N], t, a[i + j * N]);
+                }
+                a[k + k * N] = __dmul_rn(-phase, sigma);
+            }
+            if (a[k + k * N] == 0.0 && info == 0) info = k + 1;
+        }
+    }
+
+    // qr.jl:63-89: Q' r by the reflectors, then R x = Q' r.
+    __device__ __forceinline__ void backsolve(double (&x)[N]) const {
+#pragma unroll
+        for (int k = 0; k < N; ++k) {
+            double t = x[k];
+#pragma unroll
+            for (int i = k + 1; i < N; ++i) t = A_::madd(a[i + k * N], x[i], t);
+            t = __dmul_rn(t, tau[k]);
+            x[k] = __dsub_rn(x[k], t);
+#pragma unroll
+            for (int i = k + 1; i < N; ++i) x[i] = A_::msub(a[i + k * N], t, x[i]);
+        }
+#pragma unroll
+        for (int k = N - 1; k >= 0; --k) {
+            const double xk = __ddiv_rn(x[k], a[k + k * N]);
+            x[k] = xk;
+#pragma unroll
+            for (int i = 0; i < k; ++i) x[i] = A_::msub(a[i + k * N], xk, x[i]);
+        }
+    }
+
+    // The same-type ldiv!! (factors.jl:931-936), as LUFactor's Float64 branch.
+    __device__ __forceinline__ void ldiv(const double (&r)[N], double (&d)[N]) const {
+        int k = rhs_exponent<N>(r, e);
+        double x[N];
+#pragma unroll
+        for (int i = 0; i < N; ++i) x[i] = k == 0 ? r[i] : scale2_in(r[i], -k);  // -k in [-6, 1023]
+        backsolve(x);
+        int e2 = k - e;
+#pragma unroll
+        for (int i = 0; i < N; ++i) d[i] = e2 == 0 ? x[i] : scale2_in(x[i], e2);  // e2 in [0, 1029]
+    }
+};
+
 // The Float64 factorisation of the mixed step's rare branches (a promoted system, or the
 // promotion of a failed Float32 step), with its matrix in thread-local memory instead of
 // registers: the same operations in the same order as LUFactor<F, N, double> (lu.jl:24-64,
@@ -380,7 +498,9 @@ template <bool F, int N> struct LocalLU {
 // PlainRef: the plain (TF = T) step refines its direction (Refinement with a Float64 factor), a
 // rare configuration kept in its own instantiation so the common plain step holds no refinement
 // state in registers.
-template <class Fam, bool F, bool Mixed, bool PlainRef = false> struct Solver {
+// Qr selects the static Householder QR for the plain step's factor (QRFactorization with a
+// Float64 factor), else the pivoted LU.
+template <class Fam, bool F, bool Mixed, bool PlainRef = false, bool Qr = false> struct Solver {
     static constexpr int N = Fam::N, M = Fam::M;
     using JS = typename Fam::JState;
     using A = Arith<F>;
@@ -720,7 +840,7 @@ template <class Fam, bool F, bool Mixed, bool PlainRef = false> struct Solver {
         double merit = st.merit;
         constexpr bool ref = PlainRef;
         {
-            LUFactor<F, N, double> fac;
+            typename std::conditional<Qr, QRFactor<F, N>, LUFactor<F, N, double>>::type fac;
             park_x(x);
             // grad_ratio_and_norm from the sums that the factor's load folds; its scaled
             // branches, for sums out of range, run in full once the factor is done with

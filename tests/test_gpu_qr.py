@@ -1,0 +1,85 @@
+"""Newton with QRFactorization on square batches: the static Householder QR factor
+(src/linear/static/qr.jl:9-89) in the one-thread kernel, against the oracle's restatement of the
+same factor. The bar is the batch contract: bit for bit under the unfused arithmetic; identical
+codes and iteration counts and 1e-10 relative error under the fused one.
+"""
+
+import numpy as np
+import pytest
+
+from test_gpu_parity import NAMES, OPTS, check_parity, run_gpu
+from workloads import cubic_affine, cubic_affine_illcond, cubic_affine_pivoting
+
+pytestmark = pytest.mark.gpu
+
+
+def qr_newton(gsb, arith, glob="backtracking"):
+    g = gsb.Backtracking() if glob == "backtracking" else gsb.Static()
+    return gsb.Newton(linsolve=gsb.QRFactorization(), globalization=g, arithmetic=arith)
+
+
+@pytest.mark.parametrize("arith", ["fused", "unfused"])
+@pytest.mark.parametrize("n", [2, 3, 4, 6, 8])
+def test_qr_parity(gsb, oracle, n, arith):
+    X0, P = cubic_affine(n, 30000, n + 1.0, 40 + n)
+    prob = gsb.NonlinearProblem(gsb.CubicAffine(n))
+    m = qr_newton(gsb, arith)
+    opts = gsb.Options(**OPTS)
+    xg, sg = run_gpu(gsb, prob, m, X0, P, opts)
+    xo, so = oracle.solve_batch(prob, m, X0.copy(), P, opts)
+    check_parity(xg, sg, xo, so, bitwise=(arith == "unfused"))
+    assert np.all(so["code"] == 0)
+
+
+@pytest.mark.parametrize("n", [4, 8])
+def test_qr_hard_systems(gsb, oracle, n):
+    # pivoting-heavy and ill-conditioned Jacobians (cond 1e3..1e9), Static and Backtracking:
+    # several outcomes, and the reflector branches (zero subcolumns, negative x_1) exercised
+    X0, P = cubic_affine_pivoting(n, 4096, 0.5, 41)
+    X1, P1 = cubic_affine_illcond(n, 4096, 42)
+    X0, P = np.concatenate([X0, X1]), np.concatenate([P, P1])
+    prob = gsb.NonlinearProblem(gsb.CubicAffine(n))
+    opts = gsb.Options(**OPTS)
+    for glob in ("static", "backtracking"):
+        m = qr_newton(gsb, "unfused", glob)
+        xg, sg = run_gpu(gsb, prob, m, X0, P, opts)
+        xo, so = oracle.solve_batch(prob, m, X0.copy(), P, opts)
+        check_parity(xg, sg, xo, so, bitwise=True)
+    assert len(np.unique(so["code"])) >= 2
+
+
+def test_qr_six_outcomes_singular_and_order(gsb, oracle):
+    codes = [1, 2, 3, 4, 5, 6, 1, 3]
+    X0 = np.array([[2.5, 3.5]] * 8)
+    P = np.array(codes, float)[:, None]
+    prob = gsb.NonlinearProblem(gsb.Hetero6())
+    m = qr_newton(gsb, "unfused")
+    opts = gsb.Options(max_iterations=3)
+    xg, sg = run_gpu(gsb, prob, m, X0, P, opts)
+    xo, so = oracle.solve_batch(prob, m, X0.copy(), P, opts)
+    assert sg.tobytes() == so.tobytes() and xg.tobytes() == xo.tobytes()
+    assert "SINGULAR" in [NAMES[c] for c in sg["code"]]
+    p = np.array([[2.125, 1.5], [1.25, 2.0], [1.5, 2.5], [1.75, 3.0]])
+    x0 = np.array([[2.0, 1.0], [4.0, 4.0], [3.5, 2.5], [4.0, 3.0]])
+    prob2 = gsb.NonlinearProblem(gsb.Coupled2())
+    o2 = gsb.Options(max_iterations=60)
+    xg2, sg2 = run_gpu(gsb, prob2, m, x0, p, o2)
+    xo2, so2 = oracle.solve_batch(prob2, m, x0.copy(), p, o2)
+    assert sg2.tobytes() == so2.tobytes() and xg2.tobytes() == xo2.tobytes()
+    xp, sp = run_gpu(gsb, prob2, m, x0, p, o2, order=[3, 1, 0, 2])
+    assert sp.tobytes() == sg2.tobytes() and xp.tobytes() == xg2.tobytes()
+
+
+def test_qr_refusals(gsb):
+    # the device QR step is Float64 without refinement; other forms are refused before a launch
+    X0, P = cubic_affine(4, 64, 5.0, 43)
+    prob = gsb.NonlinearProblem(gsb.CubicAffine(4))
+    opts = gsb.Options(**OPTS)
+    for m in (gsb.Newton(linsolve=gsb.QRFactorization("float32"), refinement=gsb.Refinement()),
+              gsb.Newton(linsolve=gsb.QRFactorization(), refinement=gsb.Refinement())):
+        with pytest.raises(gsb.ArgumentError, match="Float64 factor and no refinement"):
+            run_gpu(gsb, prob, m, X0, P, opts)
+    X12, P12 = cubic_affine(12, 64, 13.0, 43)
+    with pytest.raises(gsb.ArgumentError, match="no batch kernel"):
+        run_gpu(gsb, gsb.NonlinearProblem(gsb.CubicAffine(12)), gsb.Newton(
+            linsolve=gsb.QRFactorization()), X12, P12, opts)

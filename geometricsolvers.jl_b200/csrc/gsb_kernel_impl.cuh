@@ -259,24 +259,30 @@ __global__ void __launch_bounds__(kThreads) team_kernel(const __grid_constant__ 
     });
 }
 
-// The least-squares form: one Levenberg–Marquardt solve per thread. Shared memory holds each
-// system's M observations (odd row stride) and, after the rows, the M abscissae of the batch.
+// The least-squares form: one Levenberg–Marquardt solve per thread, with the thread's
+// observations in a shared-memory row and the abscissae shared by the CTA. Iteration counts
+// differ widely between systems (in the exponential-sum batch about half run to max_iterations
+// while the rest converge early) and a warp steps as long as its slowest lane, so the grid holds
+// the resident CTAs only, each CTA works through a contiguous range of systems, and a lane whose
+// system closes stores it and takes the range's next system from a shared-memory counter. Each
+// system's solve is the same sequence of steps as a solve of its own.
 template <class Fam, bool F, bool Mixed>
 __global__ void __launch_bounds__(kThreads, 3) lm_kernel(const __grid_constant__ GsbMethod m,
                                  const __grid_constant__ GsbOptions o,
                                  const __grid_constant__ Launch L) {
     extern __shared__ double smem[];
+    __shared__ unsigned long long next;
     constexpr int N = Fam::N, M = Fam::M, RS = (M % 2 == 1) ? M : M + 1;
     const int tid = threadIdx.x;
-    const int64_t base = (int64_t)blockIdx.x * blockDim.x;
-    const int64_t i = base + tid;
+    const int64_t chunk = (L.nsys + gridDim.x - 1) / gridDim.x;
+    const int64_t lo = (int64_t)blockIdx.x * chunk;
+    const int64_t count = (L.nsys - lo < chunk ? L.nsys - lo : chunk);
+    if (count <= 0) return;  // the whole CTA
     double* prow = smem + tid * RS;
     double* tsh = smem + kThreads * RS;
     for (int k = tid; k < M; k += blockDim.x) tsh[k] = __ldg(L.shared + k);
-    if (L.order == nullptr && L.p_layout == GSB_AOS) {
-        stage_aos<M, RS, kThreads>(smem, L.P + base * M, L.nsys - base, tid);
-    } else if (i < L.nsys) {
-        const int64_t idx = L.order ? L.order[i] - L.order_base : i;
+    auto index = [&](int64_t i) { return L.order ? L.order[i] - L.order_base : i; };
+    auto load_row = [&](int64_t idx) {
         if (L.p_layout == GSB_SOA) {
 #pragma unroll 4
             for (int k = 0; k < M; ++k) prow[k] = __ldg(L.P + (int64_t)k * L.nsys + idx);
@@ -284,26 +290,50 @@ __global__ void __launch_bounds__(kThreads, 3) lm_kernel(const __grid_constant__
 #pragma unroll 4
             for (int k = 0; k < M; ++k) prow[k] = __ldg(L.P + idx * M + k);
         }
+    };
+    // the range's first kThreads systems, staged together
+    const int64_t first = count < kThreads ? count : kThreads;
+    if (L.order == nullptr && L.p_layout == GSB_AOS) {
+        stage_aos<M, RS, kThreads>(smem, L.P + lo * M, first, tid);
+    } else if (tid < first) {
+        load_row(index(lo + tid));
     }
+    if (tid == 0) next = (unsigned long long)first;
     __syncthreads();
-    if (i >= L.nsys) return;
-    const int64_t idx = L.order ? L.order[i] - L.order_base : i;
     Fam fam{prow, tsh};
-    double x[N];
-#pragma unroll
-    for (int k = 0; k < N; ++k)
-        x[k] = L.x_layout == GSB_SOA ? L.X[(int64_t)k * L.nsys + idx] : L.X[idx * N + k];
     LMSolver<Fam, F, Mixed> sv(fam, m, o);
-    double gr;
-    DevStatus s = sv.solve(x, gr);
+    typename LMSolver<Fam, F, Mixed>::Run run;
+    double x[N];
+    auto start = [&](int64_t idx) {
 #pragma unroll
-    for (int k = 0; k < N; ++k) {
-        if (L.x_layout == GSB_SOA) L.X[(int64_t)k * L.nsys + idx] = x[k];
-        else L.X[idx * N + k] = x[k];
+        for (int k = 0; k < N; ++k)
+            x[k] = L.x_layout == GSB_SOA ? L.X[(int64_t)k * L.nsys + idx] : L.X[idx * N + k];
+        sv.begin(x, run);
+    };
+    bool active = tid < first;
+    int64_t idx = active ? index(lo + tid) : 0;
+    if (active) start(idx);
+    while (true) {
+        while (active && run.done) {
+#pragma unroll
+            for (int k = 0; k < N; ++k) {
+                if (L.x_layout == GSB_SOA) L.X[(int64_t)k * L.nsys + idx] = x[k];
+                else L.X[idx * N + k] = x[k];
+            }
+            if (L.s_kind == GSB_STATUS64) store_status(L.S, idx, run.s, run.gr);
+            else reinterpret_cast<unsigned char*>(L.S)[idx] = (unsigned char)run.s.code;
+            if (L.tally) tally_code(L.tally, run.s.code);
+            const long long q = (long long)atomicAdd(&next, 1ull);
+            active = q < count;
+            if (active) {
+                idx = index(lo + q);
+                load_row(idx);
+                start(idx);
+            }
+        }
+        if (!active) break;
+        sv.iterate(x, run);
     }
-    if (L.s_kind == GSB_STATUS64) store_status(L.S, idx, s, gr);
-    else reinterpret_cast<unsigned char*>(L.S)[idx] = (unsigned char)s.code;
-    if (L.tally) tally_code(L.tally, s.code);
 }
 
 // The warp form (n = 12 ... 32): T lanes per system, kThreads / T systems per CTA. Each system's
@@ -370,6 +400,7 @@ struct KernelEntry {
     int smem_doubles;  // dynamic shared memory of a CTA, in doubles
     int systems_per_block;
     bool attr_set[64];
+    bool resident = false;  // fn works through ranges of systems: launch the resident CTAs only
 };
 
 template <class Fam, bool F, bool Mixed, bool PlainRef> KernelEntry* entry() {
@@ -391,7 +422,7 @@ template <class Fam, bool F> KernelEntry* qr_entry() {
 
 template <class Fam, bool F, bool Mixed> KernelEntry* lm_entry() {
     constexpr int RS = (Fam::M % 2 == 1) ? Fam::M : Fam::M + 1;
-    static KernelEntry e{lm_kernel<Fam, F, Mixed>, nullptr, kThreads * RS + Fam::M, kThreads, {}};
+    static KernelEntry e{lm_kernel<Fam, F, Mixed>, nullptr, kThreads * RS + Fam::M, kThreads, {}, true};
     return &e;
 }
 

@@ -401,6 +401,25 @@ int select_entry(const GsbProblem* prob, const GsbMethod* method, KernelEntry** 
     return 0;
 }
 
+// The grid of a launch: one CTA per kernel-sized chunk of systems, or, for a kernel that works
+// through ranges of systems, at most the CTAs that are resident on the device at once.
+int launch_blocks(const KernelEntry* ke, int64_t nsys, size_t smem, int64_t* blocks) {
+    *blocks = (nsys + ke->systems_per_block - 1) / ke->systems_per_block;
+    if (!ke->resident) return 0;
+    int dev = 0, sms = 0, occ = 0;
+    if (int rc = cuda_err(cudaGetDevice(&dev), "cudaGetDevice")) return rc;
+    if (int rc = cuda_err(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev),
+                          "cudaDeviceGetAttribute"))
+        return rc;
+    if (int rc = cuda_err(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                              &occ, reinterpret_cast<const void*>(ke->fn), kThreads, smem),
+                          "cudaOccupancyMaxActiveBlocksPerMultiprocessor"))
+        return rc;
+    const int64_t cap = (int64_t)(sms > 0 ? sms : 1) * (occ > 0 ? occ : 1);
+    if (*blocks > cap) *blocks = cap;
+    return 0;
+}
+
 int launch_solve(const GsbProblem* prob, const GsbMethod* method, const GsbOptions* opt, double* X,
                  int32_t x_layout, void* S, int32_t s_kind, const double* P, int32_t p_layout,
                  const int64_t* order, int32_t order_base, int64_t nsys, cudaStream_t st,
@@ -419,7 +438,8 @@ int launch_solve(const GsbProblem* prob, const GsbMethod* method, const GsbOptio
         ke->attr_set[dev & 63] = true;
     }
     Launch L{X, x_layout, S, s_kind, P, p_layout, order, order_base, nsys, prob->shared, tally_dev};
-    int64_t blocks = (nsys + ke->systems_per_block - 1) / ke->systems_per_block;
+    int64_t blocks = 0;
+    if (int rc = launch_blocks(ke, nsys, smem, &blocks)) return rc;
     ke->fn<<<(unsigned)blocks, kThreads, smem, st>>>(*method, *opt, L);
     return cuda_err(cudaGetLastError(), "kernel launch");
 }
@@ -546,7 +566,8 @@ int gsb_solve_batch(const GsbProblem* prob, const GsbMethod* method, const GsbOp
     }
     Launch L{X, x_layout, S, s_kind, P, p_layout, order, order_base, nsys, prob->shared,
              ws ? ws->tally : nullptr};
-    int64_t blocks = (nsys + ke->systems_per_block - 1) / ke->systems_per_block;
+    int64_t blocks = 0;
+    if (int rc = launch_blocks(ke, nsys, smem, &blocks)) return rc;
     ke->fn<<<(unsigned)blocks, kThreads, smem, st>>>(*method, *opt, L);
     if (int rc = cuda_err(cudaGetLastError(), "kernel launch")) return rc;
     if (tally) {

@@ -748,14 +748,24 @@ template <class Fam, bool F, bool Mixed = false> struct LMSolver {
 
     // solve!!, src/nonlinear/solver.jl:277-378, with the least-squares branches (stationarity,
     // re-measured diagnostics, the discarded step of keeps_step_start, solver.jl:183-189 and
-    // 330-339). `gr` receives the gradratio of the last diagnostics (newton_finish!!).
-    __device__ DevStatus solve(double (&x)[N], double& gr) const {
+    // 330-339), as a run that advances one step at a time: `begin` takes the start (and may
+    // already close the run), each `iterate` one pass of the loop; `done` marks the close.
+    // `gr` is the gradratio of the last diagnostics (newton_finish!!).
+    struct Run {
         State st;
+        DevStatus s;
+        double ftest0, gr;
+        int stalls;
+        bool done;
+    };
+
+    __device__ void begin(double (&x)[N], Run& r) const {
+        State& st = r.st;
+        DevStatus& s = r.s;
         fnorms(x, st.fnorm, st.fmax);
         st.mu = m.lm_mu0;
         st.gradratio = kNaN;
         st.jnorm = 0.0;
-        DevStatus s;
         s.code = SUCCESS;
         s.iterations = 0;
         s.fnorm = st.fnorm;
@@ -765,102 +775,117 @@ template <class Fam, bool F, bool Mixed = false> struct LMSolver {
         s.stationary = false;
         s.rate = kNaN;
         s.contracted = false;
-        gr = kNaN;
+        r.gr = kNaN;
+        r.stalls = 0;
+        r.done = true;
         if (!isfin(st.fnorm)) {
             close(s, NONFINITE, false, false);
-            return s;
+            return;
         }
-        const double ftest0 = o.norm == 1 ? st.fmax : st.fnorm;
-        if (residual_converged(s, ftest0, ftest0)) return s;
+        r.ftest0 = o.norm == 1 ? st.fmax : st.fnorm;
+        if (residual_converged(s, r.ftest0, r.ftest0)) return;
         if (o.max_iterations == 0) {
             close(s, MAXITERS, false, false);
-            return s;
+            return;
         }
-        int stalls = 0;
-        while (true) {
-            double xk[N];
+        r.done = false;
+    }
+
+    __device__ void iterate(double (&x)[N], Run& r) const {
+        State& st = r.st;
+        DevStatus& s = r.s;
+        const double ftest0 = r.ftest0;
+        r.done = true;
+        double xk[N];
 #pragma unroll
-            for (int i = 0; i < N; ++i) xk[i] = x[i];
-            const DevStatus sk = s;
-            StepInfo info;
-            step(st, x, info);
-            record(s, info);
-            const State st_step = st;
-            gr = st.gradratio;
-            if (info.code == SINGULAR || info.code == NONFINITE || info.code == MAXITERS) return s;
-            if (info.code == LINESEARCH_FAILED && info.stepnorm == 0.0 && !stationary(st, s))
-                return s;
-            if (residual_converged(s, o.norm == 1 ? st.fmax : s.fnorm, ftest0)) {
-                close(s, SUCCESS, false, false);
-                return s;
-            }
-            bool refreshed = false;
+        for (int i = 0; i < N; ++i) xk[i] = x[i];
+        const DevStatus sk = s;
+        StepInfo info;
+        step(st, x, info);
+        record(s, info);
+        const State st_step = st;
+        r.gr = st.gradratio;
+        if (info.code == SINGULAR || info.code == NONFINITE || info.code == MAXITERS) return;
+        if (info.code == LINESEARCH_FAILED && info.stepnorm == 0.0 && !stationary(st, s)) return;
+        if (residual_converged(s, o.norm == 1 ? st.fmax : s.fnorm, ftest0)) {
+            close(s, SUCCESS, false, false);
+            return;
+        }
+        bool refreshed = false;
+        if (stationary(st, s)) {
+            refresh(st, x);
+            refreshed = true;
+            r.gr = st.gradratio;
             if (stationary(st, s)) {
-                refresh(st, x);
-                refreshed = true;
-                gr = st.gradratio;
-                if (stationary(st, s)) {
-                    close(s, SUCCESS, true, false);
-                    return s;
-                }
-                if (sk.iterations >= 1 && s.fnorm >= sk.fnorm && stationary(st_step, sk)) {
-                    // discarded_step_status, solver.jl:103-109
+                close(s, SUCCESS, true, false);
+                return;
+            }
+            if (sk.iterations >= 1 && s.fnorm >= sk.fnorm && stationary(st_step, sk)) {
+                // discarded_step_status, solver.jl:103-109
 #pragma unroll
-                    for (int i = 0; i < N; ++i) x[i] = xk[i];
-                    const int failures = s.step_failures;
-                    const bool promoted = s.promoted;
-                    s = sk;
-                    s.code = SUCCESS;
-                    s.step_failures = failures;
-                    s.promoted = promoted;
-                    s.stationary = true;
-                    s.contracted = false;
-                    gr = st_step.gradratio;
-                    return s;
-                }
-            }
-            const bool steptested = !(info.code == STALLED || info.limited);
-            const double xnorm = steptested ? rnorm<F, N>(x) : kNaN;
-            bool contracted = false;
-            if (!info.shortened && o.rate_test && s.iterations >= o.min_iterations) {
-                const double th = jmax(s.rate, sk.rate);
-                if (s.stepnorm > 0.0 && th < 1.0)
-                    contracted = A::mul(__ddiv_rn(th, A::sub(1.0, th)), s.stepnorm) <=
-                                 A::mul(o.kappa, jmax(o.x_abstol, A::mul(o.x_reltol, xnorm)));
-            }
-            bool stepc = false;
-            if (steptested && s.iterations >= o.min_iterations) {
-                stepc = s.iterations > 0 && s.stepnorm > 0.0 &&
-                        s.stepnorm <= jmax(o.x_abstol, A::mul(o.x_reltol, xnorm));
-                stepc = stepc || (info.code == SUCCESS && info.stepnorm == 0.0);
-                stepc = stepc || (o.roundoff && s.rate >= 1.0 && sk.rate < 1.0);
-            }
-            if (contracted || stepc) {
-                if (!refreshed) {
-                    refresh(st, x);
-                    gr = st.gradratio;
-                }
-                if (stationary(st, s)) {
-                    close(s, SUCCESS, true, false);
-                    return s;
-                }
-                close(s, contracted ? SUCCESS : STALLED, false, contracted);
-                return s;
-            }
-            if (info.code == STALLED) {
-                stalls += 1;
-                if (stalls >= o.max_stalls) {
-                    close(s, STALLED, false, false);
-                    return s;
-                }
-            } else {
-                stalls = 0;
-            }
-            if (s.iterations >= o.max_iterations) {
-                close(s, MAXITERS, false, false);
-                return s;
+                for (int i = 0; i < N; ++i) x[i] = xk[i];
+                const int failures = s.step_failures;
+                const bool promoted = s.promoted;
+                s = sk;
+                s.code = SUCCESS;
+                s.step_failures = failures;
+                s.promoted = promoted;
+                s.stationary = true;
+                s.contracted = false;
+                r.gr = st_step.gradratio;
+                return;
             }
         }
+        const bool steptested = !(info.code == STALLED || info.limited);
+        const double xnorm = steptested ? rnorm<F, N>(x) : kNaN;
+        bool contracted = false;
+        if (!info.shortened && o.rate_test && s.iterations >= o.min_iterations) {
+            const double th = jmax(s.rate, sk.rate);
+            if (s.stepnorm > 0.0 && th < 1.0)
+                contracted = A::mul(__ddiv_rn(th, A::sub(1.0, th)), s.stepnorm) <=
+                             A::mul(o.kappa, jmax(o.x_abstol, A::mul(o.x_reltol, xnorm)));
+        }
+        bool stepc = false;
+        if (steptested && s.iterations >= o.min_iterations) {
+            stepc = s.iterations > 0 && s.stepnorm > 0.0 &&
+                    s.stepnorm <= jmax(o.x_abstol, A::mul(o.x_reltol, xnorm));
+            stepc = stepc || (info.code == SUCCESS && info.stepnorm == 0.0);
+            stepc = stepc || (o.roundoff && s.rate >= 1.0 && sk.rate < 1.0);
+        }
+        if (contracted || stepc) {
+            if (!refreshed) {
+                refresh(st, x);
+                r.gr = st.gradratio;
+            }
+            if (stationary(st, s)) {
+                close(s, SUCCESS, true, false);
+                return;
+            }
+            close(s, contracted ? SUCCESS : STALLED, false, contracted);
+            return;
+        }
+        if (info.code == STALLED) {
+            r.stalls += 1;
+            if (r.stalls >= o.max_stalls) {
+                close(s, STALLED, false, false);
+                return;
+            }
+        } else {
+            r.stalls = 0;
+        }
+        if (s.iterations >= o.max_iterations) {
+            close(s, MAXITERS, false, false);
+            return;
+        }
+        r.done = false;
+    }
+
+    __device__ DevStatus solve(double (&x)[N], double& gr) const {
+        Run r;
+        begin(x, r);
+        while (!r.done) iterate(x, r);
+        gr = r.gr;
+        return r.s;
     }
 };
 

@@ -442,13 +442,30 @@ template <class Fam, int T, bool F, bool Mixed, bool PlainRef> struct WarpSolver
     // grad_ratio_and_norm, src/nonlinear/newton.jl:1287-1298.
     __device__ void grad_ratio_and_norm(const JS& js, double Fl, double fnorm, double& gr,
                                         double& jnorm) const {
-        // ‖J‖_F as the column-major left fold: every lane folds all entries
         double s = 0.0;
-        for (int k = 0; k < N; ++k) {
-            const double dk = fam.template col_diag<T>(tm, js, k);
-            for (int i = 0; i < N; ++i) {
-                const double v = fam.Jall(js, i, k, dk);
-                s = (i == 0 && k == 0) ? A::mul(v, v) : A::madd(v, v, s);
+        if constexpr (F) {
+            // Under the fused arithmetic (whose FMAs already round this sum apart from the
+            // reference's) each lane folds its own row and the lanes combine in a butterfly,
+            // which leaves the same bits in every lane: N + log2(T) dependent steps instead of
+            // N^2. ‖J‖_F feeds only the reported gradient ratio.
+            if (tm.lane < N) {
+                const int i = tm.lane;
+                const double v0 = fam.Jent(js, i, 0);
+                s = A::mul(v0, v0);
+                for (int k = 1; k < N; ++k) {
+                    const double v = fam.Jent(js, i, k);
+                    s = A::madd(v, v, s);
+                }
+            }
+            s = tm.sum(s);
+        } else {
+            // ‖J‖_F as the column-major left fold: every lane folds all entries
+            for (int k = 0; k < N; ++k) {
+                const double dk = fam.template col_diag<T>(tm, js, k);
+                for (int i = 0; i < N; ++i) {
+                    const double v = fam.Jall(js, i, k, dk);
+                    s = (i == 0 && k == 0) ? A::mul(v, v) : A::madd(v, v, s);
+                }
             }
         }
         double mx = 0.0;

@@ -9,7 +9,7 @@ the explicit stage guess plus a learned correction. It is trained on the device,
 project's own forward and backward kernels and Adam, on solutions that the plain Newton solver
 produced. At solve time the prediction is kept for a system only where its FP64 residual norm
 beats the default start's (``gsb_warm_start_select``), so plain Newton stays both the fallback
-and the judge of every prediction.
+and the arbiter of every prediction.
 """
 
 from __future__ import annotations

@@ -41,7 +41,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="gsb200", choices=["gsb200", "reference"])
     ap.add_argument("--nsys", type=int, default=NSYS)
-    ap.add_argument("--profile", choices=["plain", "mixed", "lm", "irk", "mlp", "shared"],
+    ap.add_argument("--profile", choices=["plain", "mixed", "lm", "irk", "mlp", "predict", "shared"],
                     default=None,
                     help="run `--warmup` + `--steps` solves of one form only (for ncu captures): "
                          "the cubic-affine batch of size --n, or the exponential-sum fit (lm)")
@@ -472,6 +472,19 @@ def run_profile(args):
 
     import gsb200 as G
 
+    if args.profile == "predict":
+        # the warm-start network's prediction for args.nsys states (untrained weights)
+        from workloads import c3_states
+
+        net = G.MlpWarmStart(G.IrkHenonHeiles(0.1), seed=0)
+        st_h = c3_states(args.nsys, stream=1)
+        net.set_normalisation(st_h, net.stage_guess(st_h))
+        S_ = torch.tensor(st_h, device="cuda")
+        ms = _events_ms(lambda: net.predict(S_), args.steps, args.warmup,
+                        torch.cuda.current_stream())
+        print(json.dumps({"profile": "predict", "nsys": args.nsys, "ms_per_step": ms,
+                          "err": int(net.err.item())}))
+        return
     if args.profile == "mlp":
         # gradient steps of the warm-start network on args.nsys states (random targets)
         from workloads import c3_states
@@ -650,6 +663,19 @@ def run_c3(args, opts, hbm_peak, hbm_src, peaks):
             forms[name] = {"systems_per_s": float(np.sum(ok)) / (ms * 1e-3), "ms_per_step": ms,
                            "solved": int(np.sum(ok)), "mean_iterations": float(st["iterations"].mean()),
                            "fp64_oracle_max_rel_err": float(err.max())}
+        # where the warm step's time goes: the network's prediction, the accept-if-better gate
+        # and the Newton solve from the chosen starts
+        Z0 = net.predict(P)
+        Zs, _ = net.select(P, Z0, X0)
+
+        def solve_from_warm():
+            Xw.copy_(Zs)
+            G.solve_batch(Xw, S, prob, plain, ps, options=opts)
+
+        forms["mlp_warm_start"]["phases_ms"] = {
+            "predict": _events_ms(lambda: net.predict(P), args.steps, args.warmup, stream),
+            "select": _events_ms(lambda: net.select(P, Z0, X0), args.steps, args.warmup, stream),
+            "solve": _events_ms(solve_from_warm, args.steps, args.warmup, stream)}
     clocks = clk.summary()
     forms["mlp_warm_start"]["fallback_rate"] = 1.0 - float(acc_last["acc"].float().mean().item())
     forms["mlp_warm_start"]["training"] = {"samples": ntr, "epochs": 80, "batch": 8192,

@@ -21,6 +21,16 @@ constexpr uint32_t kWaitLimit = 1u << 26;  // mbarrier polls before a tile gives
 __device__ __forceinline__ uint16_t bf16_bits(float v) {
     return __bfloat16_as_ushort(__float2bfloat16_rn(v));
 }
+// Two values rounded to BF16 (nearest even), the first in the low half.
+__device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
+    return (uint32_t)bf16_bits(lo) | ((uint32_t)bf16_bits(hi) << 16);
+}
+// 16 bytes into a tile at byte offset `off` (a multiple of 16).
+__device__ __forceinline__ void store16(uint16_t* tile, uint32_t off, const uint32_t (&w)[4]) {
+    asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(umma::smem_u32(tile) + off),
+                 "r"(w[0]), "r"(w[1]), "r"(w[2]), "r"(w[3])
+                 : "memory");
+}
 
 // ─── self-test of the tile product ─────────────────────────────────────────────────────────
 // D (128 x N, FP32) = A B^T for a 128 x K A and an N x K B (mode 0, both K-major), or with A
@@ -193,7 +203,7 @@ __device__ __forceinline__ void tiles_ready() {
 }
 
 // Wait for the MMAs committed so far; false (and the CTA's failure flag) on a timeout.
-__device__ __forceinline__ bool mma_done(NetSmem& S, uint32_t& phase) {
+template <class Smem> __device__ __forceinline__ bool mma_done(Smem& S, uint32_t& phase) {
     const bool ok = umma::mbar_wait(&S.mbar, phase & 1u, kWaitLimit);
     phase += 1;
     umma::fence_after_sync();
@@ -278,35 +288,123 @@ __device__ __forceinline__ void stage_guess(const double* y, const double* share
     }
 }
 
+// Shared memory of an inference CTA: the two weight tiles, one activation tile (H1, then H2 once
+// the layer-2 product has read H1), the small FP32 parameters and the barrier state — about
+// 72 KB, so that three CTAs share an SM where the training layout (182 KB) fits one. Layer 3's
+// accumulator reuses TMEM columns 0..15 once layer 2's have been read, so a CTA holds 128 columns.
+struct InferSmem {
+    uint16_t w2t[128 * 128];  // B of layer 2: N = out, K = in
+    uint16_t w3t[16 * 128];   // B of layer 3: N = 16, K = in
+    uint16_t h[128 * 128];    // A of layer 2 (H1), then A of layer 3 (H2)
+    float w1[512], b1[128], b2[128], b3[16];
+    uint64_t mbar;
+    uint32_t tmem;
+    int failed;
+};
+
 // Inference: Z0 = guess + scale * net(y), persistent over 128-system tiles.
 __global__ void __launch_bounds__(128) net_predict(const float* theta, const uint16_t* pack,
                                                    const float* norm, const double* shared,
                                                    const double* states, double* Z0, int64_t n,
                                                    int* err) {
     extern __shared__ __align__(1024) unsigned char smraw[];
-    NetSmem& S = *reinterpret_cast<NetSmem*>(smraw);
-    net_setup(S, theta, pack, false, 256);
-    uint32_t phase = 0;
+    InferSmem& S = *reinterpret_cast<InferSmem*>(smraw);
     const int t = threadIdx.x;
+    stage_tile(S.w2t, pack + kPW2T, 128, 128);
+    stage_tile(S.w3t, pack + kPW3T, 16, 128);
+    for (int q = t; q < 512; q += blockDim.x) S.w1[q] = theta[kW1 + q];
+    for (int q = t; q < 128; q += blockDim.x) {
+        S.b1[q] = theta[kB1 + q];
+        S.b2[q] = theta[kB2 + q];
+    }
+    if (t < 16) S.b3[t] = theta[kB3 + t];
+    if (t == 0) {
+        S.failed = 0;
+        umma::mbar_init(&S.mbar, 1);
+    }
+    if (t < 32) umma::tmem_alloc(&S.tmem, 128);
+    tiles_ready();
+    const uint32_t tm = S.tmem;
+    const uint32_t lb = umma::lane_base(tm);
+    uint32_t phase = 0;
     for (int64_t tile = blockIdx.x; tile * 128 < n; tile += gridDim.x) {
         const int64_t row = tile * 128 + t;
         const bool active = row < n;
         float xh[4];
         normalise(states + (active ? row : 0) * 4, norm, active, xh);
+        // layer 1 on the CUDA cores, H1 into the activation tile: the eight columns of a
+        // core-matrix row are 16 contiguous bytes, one store (a warp's 32 rows fill 512
+        // contiguous bytes, no bank conflict)
+        for (int jc = 0; jc < 16; ++jc) {
+            uint32_t w[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                float g[2];
+#pragma unroll
+                for (int u = 0; u < 2; ++u) {
+                    const int j = jc * 8 + 2 * q + u;
+                    float z = S.b1[j];
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) z = fmaf(S.w1[j * 4 + i], xh[i], z);
+                    g[u] = active ? gelu(z) : 0.0f;
+                }
+                w[q] = pack_bf16x2(g[0], g[1]);
+            }
+            store16(S.h, umma::tile_offset(128, t, jc * 8), w);
+        }
+        tiles_ready();
+        if (t == 0) {
+            const uint32_t a0 = umma::smem_u32(S.h), b0 = umma::smem_u32(S.w2t);
+            const uint32_t id = umma::idesc_bf16(128, 128, 0, 0);
+            for (int s = 0; s < 8; ++s)
+                umma::mma(tm, umma::desc_kmajor(a0, 128, s), umma::desc_kmajor(b0, 128, s), id, s > 0);
+            umma::commit(&S.mbar);
+        }
+        if (!mma_done(S, phase)) break;
+        // H2 over H1 (the product that read H1 has completed)
+        for (int c = 0; c < 128; c += 16) {
+            float v[16];
+            umma::ld16(lb + (uint32_t)c, v);
+#pragma unroll
+            for (int h8 = 0; h8 < 2; ++h8) {
+                uint32_t w[4];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const int i0 = h8 * 8 + 2 * q;
+                    const float g0 = active ? gelu(v[i0] + S.b2[c + i0]) : 0.0f;
+                    const float g1 = active ? gelu(v[i0 + 1] + S.b2[c + i0 + 1]) : 0.0f;
+                    w[q] = pack_bf16x2(g0, g1);
+                }
+                store16(S.h, umma::tile_offset(128, t, c + h8 * 8), w);
+            }
+        }
+        tiles_ready();
+        if (t == 0) {
+            const uint32_t a0 = umma::smem_u32(S.h), b0 = umma::smem_u32(S.w3t);
+            const uint32_t id = umma::idesc_bf16(128, 16, 0, 0);
+            for (int s = 0; s < 8; ++s)
+                umma::mma(tm, umma::desc_kmajor(a0, 128, s), umma::desc_kmajor(b0, 16, s), id, s > 0);
+            umma::commit(&S.mbar);
+        }
+        if (!mma_done(S, phase)) break;
         float out[16];
-        if (!net_forward(S, xh, active, phase, out)) break;
+        umma::ld16(lb, out);
         if (active) {
             double z[12];
             stage_guess(states + row * 4, shared, z);
 #pragma unroll
-            for (int o = 0; o < kOut; ++o) Z0[row * 12 + o] = z[o] + (double)norm[8 + o] * (double)out[o];
+            for (int o = 0; o < kOut; ++o)
+                Z0[row * 12 + o] = z[o] + (double)norm[8 + o] * (double)(out[o] + S.b3[o]);
         }
+        // every lane has read its output before the next tile's products overwrite the columns
+        umma::fence_before_sync();
         __syncthreads();
+        umma::fence_after_sync();
     }
     if (S.failed && t == 0) atomicExch(err, 1);
     umma::fence_before_sync();
     __syncthreads();
-    if (t < 32) umma::tmem_free(S.tmem, 256);
+    if (t < 32) umma::tmem_free(S.tmem, 128);
 }
 
 // Training: the mean squared error of the scaled outputs against `targets` (B x 12) and its
@@ -507,15 +605,30 @@ GSB_API int gsb_umma_selftest(const uint16_t* A, const uint16_t* B, float* D, in
 
 namespace {
 
-int net_grid(const void* fn, size_t smem, int64_t n, int* grid) {
-    int dev = 0, sms = 0, occ = 0;
+// A persistent grid: the CTAs that are resident at once, by shared memory (the device's per-SM
+// capacity and per-block reservation) and by tensor memory (512 columns per SM, `tmem_cols` per
+// CTA), at most one per 128-row tile.
+int net_grid(const void* fn, size_t smem, int64_t n, int tmem_cols, int* grid) {
+    int dev = 0, sms = 0, smem_sm = 0, reserved = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return GSB_ERR_CUDA;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return GSB_ERR_CUDA;
+    if (cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) != cudaSuccess)
+        return GSB_ERR_CUDA;
+    if (cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev) != cudaSuccess)
+        return GSB_ERR_CUDA;
     if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return GSB_ERR_CUDA;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, 128, smem) != cudaSuccess) return GSB_ERR_CUDA;
+    // the largest shared-memory carveout, so that the CTAs that fit by shared memory are resident
+    if (cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             (int)cudaSharedmemCarveoutMaxShared) != cudaSuccess)
+        return GSB_ERR_CUDA;
+    int occ = (int)((size_t)smem_sm / (smem + (size_t)reserved));
+    const int by_tmem = 512 / tmem_cols;
+    if (occ > by_tmem) occ = by_tmem;
+    if (occ > 16) occ = 16;  // 2048 threads per SM
+    if (occ < 1) occ = 1;
     const int64_t tiles = (n + 127) / 128;
-    int64_t g = (int64_t)sms * (occ > 0 ? occ : 1);
+    const int64_t g = (int64_t)sms * occ;
     *grid = (int)(tiles < g ? tiles : g);
     return 0;
 }
@@ -552,9 +665,9 @@ int gsb_mlp_predict(const float* theta, const uint16_t* pack, const float* norm,
         return GSB_ERR_ARGUMENT;
     if (n == 0) return 0;
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-    const size_t smem = sizeof(gsb::mlp::NetSmem);
+    const size_t smem = sizeof(gsb::mlp::InferSmem);
     int grid = 0;
-    if (int rc = net_grid((const void*)gsb::mlp::net_predict, smem, n, &grid)) return rc;
+    if (int rc = net_grid((const void*)gsb::mlp::net_predict, smem, n, 128, &grid)) return rc;
     cudaMemsetAsync(err_scratch, 0, sizeof(int), st);
     gsb::mlp::net_predict<<<grid, 128, smem, st>>>(theta, pack, norm, shared, states, Z0, n, err_scratch);
     if (cudaGetLastError() != cudaSuccess) return GSB_ERR_CUDA;
@@ -569,7 +682,7 @@ int gsb_mlp_grad(const float* theta, const uint16_t* pack, const float* norm, co
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
     const size_t smem = sizeof(gsb::mlp::NetSmem);
     int grid = 0;
-    if (int rc = net_grid((const void*)gsb::mlp::net_grad, smem, n, &grid)) return rc;
+    if (int rc = net_grid((const void*)gsb::mlp::net_grad, smem, n, 512, &grid)) return rc;
     cudaMemsetAsync(grad, 0, gsb::mlp::kTheta * sizeof(float), st);
     cudaMemsetAsync(loss, 0, sizeof(float), st);
     cudaMemsetAsync(err_scratch, 0, sizeof(int), st);

@@ -67,9 +67,48 @@ def methods(gsb):
 
 
 def workload(rank, nsys):
+    """Rank `rank`'s shard of the n = 8 batch: its own counter stream of the seeded generator,
+    so shards are disjoint draws and every run draws the same ones."""
     from workloads import cubic_affine
 
     return cubic_affine(N_UNKNOWNS, nsys, 6.0, 1, stream=rank)
+
+
+class Ranks:
+    """The job's ranks as the bench uses them: a barrier, and the maximum (timings) and sum
+    (solved counts) of one value over ranks. Every rank calls each in the same order; with one
+    rank they are the identity. `dev` is where the reduction tensors live (the rank's GPU under
+    NCCL, the CPU under gloo)."""
+
+    def __init__(self, world, dev=None):
+        self.world = world
+        self.dev = dev
+
+    def _reduce(self, v, op):
+        if self.world == 1:
+            return v
+        import torch
+        import torch.distributed as dist
+
+        t = torch.tensor([v], dtype=torch.float64, device=self.dev)
+        dist.all_reduce(t, op=op)
+        return float(t.item())
+
+    def barrier(self):
+        if self.world > 1:
+            import torch.distributed as dist
+
+            dist.barrier()
+
+    def max(self, v):
+        import torch.distributed as dist
+
+        return self._reduce(v, dist.ReduceOp.MAX if self.world > 1 else None)
+
+    def sum(self, v):
+        import torch.distributed as dist
+
+        return self._reduce(v, dist.ReduceOp.SUM if self.world > 1 else None)
 
 
 # ─── roofline model ──────────────────────────────────────────────────────────────────────────
@@ -263,23 +302,8 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=dev)
 
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    def max_over_ranks(v):
-        if world == 1:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
-    def sum_over_ranks(v):
-        if world == 1:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.SUM)
-        return float(t.item())
+    ranks = Ranks(world, dev)
+    barrier, max_over_ranks, sum_over_ranks = ranks.barrier, ranks.max, ranks.sum
 
     import gsb200 as G
     from oracle import oracle_py as O

@@ -313,9 +313,9 @@ template <int N, int T, bool F, class TF> struct WarpLU {
         __syncwarp(tm.mask);
         info = 0;
         piv = lane;
-        for (int k = 0; k < N; ++k) {
-            // the first largest |a_ik|, i >= k (a NaN on the diagonal keeps k; a NaN below it
-            // never wins), as a (value, index) maximum with the smaller index on ties
+        // The first largest |a_ik|, i >= k (a NaN on the diagonal keeps k; a NaN below it never
+        // wins), as a (value, index) maximum with the smaller index on ties.
+        auto pivot = [&](int k) {
             double w = -2.0;
             if (lane == k) {
                 const double v = double(fabs(at(k, k)));
@@ -334,29 +334,64 @@ template <int N, int T, bool F, class TF> struct WarpLU {
                     wi = oi;
                 }
             }
-            const int p = wi;
-            if (lane == k) piv = p;
-            if (p != k) {
+            if (lane == k) piv = wi;
+            if (wi != k) {  // rows k and wi exchanged whole, lane c taking column c
                 if (mine) {
                     const TF t = at(k, lane);
-                    at(k, lane) = at(p, lane);
-                    at(p, lane) = t;
+                    at(k, lane) = at(wi, lane);
+                    at(wi, lane) = t;
                 }
                 __syncwarp(tm.mask);
             }
+        };
+        // Two steps of the elimination per pass (the same operations on every entry, in the same
+        // order, as one step at a time): step k's multipliers and its update of column k + 1,
+        // which step k + 1's pivot search reads; step k + 1's pivot row brought up to date one
+        // entry per lane; then both updates of every other entry in one pass, one read and one
+        // write of the lane's row per entry instead of two.
+        for (int k = 0; k < N; k += 2) {
+            pivot(k);
             const TF akk = at(k, k);
-            if (akk == TF(0)) {
-                if (info == 0) info = k + 1;
-            } else {
-                const TF rk = kRecip ? TF(1) / akk : TF(0);
-                if (lane > k && lane < N) {
-                    const TF l = kRecip ? at(lane, k) * rk : at(lane, k) / akk;
-                    at(lane, k) = l;
-                    for (int j = k + 1; j < N; ++j) at(lane, j) = A::msub(l, at(k, j), at(lane, j));
-                }
-                // the reciprocal replaces the pivot for the back substitution
-                if (kRecip && lane == k) at(k, k) = rk;
+            const bool dok = akk != TF(0);
+            if (!dok && info == 0) info = k + 1;
+            const TF rk = (kRecip && dok) ? TF(1) / akk : TF(0);
+            const int k1 = k + 1;
+            if (k1 == N) {
+                if (dok && kRecip && lane == k) at(k, k) = rk;
+                __syncwarp(tm.mask);
+                break;
             }
+            if (dok && lane > k && lane < N) {
+                const TF l = kRecip ? at(lane, k) * rk : at(lane, k) / akk;
+                at(lane, k) = l;
+                at(lane, k1) = A::msub(l, at(k, k1), at(lane, k1));
+            }
+            // the reciprocal replaces the pivot for the back substitution
+            if (dok && kRecip && lane == k) at(k, k) = rk;
+            __syncwarp(tm.mask);
+            pivot(k1);
+            if (dok && lane > k1 && lane < N)
+                at(k1, lane) = A::msub(at(k1, k), at(k, lane), at(k1, lane));
+            __syncwarp(tm.mask);
+            const TF ak1 = at(k1, k1);
+            const bool dok1 = ak1 != TF(0);
+            if (!dok1 && info == 0) info = k1 + 1;
+            const TF r1 = (kRecip && dok1) ? TF(1) / ak1 : TF(0);
+            if (lane > k1 && lane < N) {
+                const TF l0 = dok ? at(lane, k) : TF(0);  // this row's step-k multiplier
+                TF l1 = TF(0);
+                if (dok1) {
+                    l1 = kRecip ? at(lane, k1) * r1 : at(lane, k1) / ak1;
+                    at(lane, k1) = l1;
+                }
+                for (int j = k1 + 1; j < N; ++j) {
+                    TF v = at(lane, j);
+                    if (dok) v = A::msub(l0, at(k, j), v);
+                    if (dok1) v = A::msub(l1, at(k1, j), v);
+                    at(lane, j) = v;
+                }
+            }
+            if (dok1 && kRecip && lane == k1) at(k1, k1) = r1;
             __syncwarp(tm.mask);
         }
     }

@@ -477,7 +477,7 @@ def main():
         },
         "e2e": {"value": e2e_value, "unit": "systems/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e,
-                "api": "gsb_solve_batch_host (pinned host X, P, S; chunks of 131,072 systems)",
+                "api": "gsb_solve_batch_host (pinned host X, P, S; chunks of 262,144 systems)",
                 "timer": "host clock around the blocking call, median of the steps"},
         "gpu_launches": args.steps,
         "roofline": roof,

@@ -1055,7 +1055,7 @@ int gsb_solve_batch_host(const GsbProblem* prob, const GsbMethod* method, const 
     if (!X || !S || !P) return set_err(GSB_ERR_ARGUMENT, "null X, S or P");
     const int64_t n = prob->n;
     const int64_t sbytes = s_kind == GSB_STATUS64 ? 72 : 1;
-    if (chunk == 0) chunk = 131072;
+    if (chunk == 0) chunk = 262144;
     if (chunk > nsys) chunk = nsys;
     int dev = 0;
     if (int rc = cuda_err(cudaGetDevice(&dev), "cudaGetDevice")) return rc;

@@ -279,7 +279,7 @@ GSB_API int gsb_solve_batch_counts_noalloc(const GsbProblem* prob, const GsbMeth
 
 /* A batch whose X, S and P live in host memory (AoS layouts; page-locked memory lets the copies
  * overlap). No counterpart in the reference's device path: the call streams the batch through
- * the device in chunks of `chunk` systems (0: 131,072), on three streams, so that the copy of
+ * the device in chunks of `chunk` systems (0: 262,144), on three streams, so that the copy of
  * chunk k+1's inputs, the solve of chunk k and the copy back of chunk k-1's iterates and statuses
  * overlap. `prob->shared` must still be a device pointer. Three device staging slots are
  * allocated on the first call on a device and kept. The call returns when every result is in

@@ -126,3 +126,28 @@ def test_lm_refinement_is_refused(gsb):
     with pytest.raises(gsb.ArgumentError):
         gsb.Newton(linsolve=gsb.QRFactorization(), globalization=gsb.LevenbergMarquardt(),
                    refinement=gsb.Refinement())
+
+
+@pytest.mark.gpu
+def test_lm_lane_refill_is_per_system(gsb):
+    # 196,608 systems on the resident CTAs: each lane solves about three systems in turn, taking
+    # the next as its last one closes. Every system's iterate and status must be the bytes that a
+    # launch small enough for one system per lane gives, and an `order` permutation of the batch
+    # (systems taken in another sequence) must change nothing either.
+    import torch
+
+    X0, Y, t = c2(196608)
+    xg, sg, (prob, m, opts) = _solve(gsb, X0, Y, t)
+    idx = np.r_[0:4096, 98304:102400, 192512:196608]
+    xs, ss, _ = _solve(gsb, X0[idx], Y[idx], t)
+    assert xs.tobytes() == xg[idx].tobytes()
+    # raw 72-byte records (indexing the structured array would not copy its padding bytes)
+    raw = np.ascontiguousarray(sg).view(np.uint8).reshape(-1, 72)
+    assert ss.tobytes() == raw[idx].tobytes()
+    perm = np.random.default_rng(3).permutation(X0.shape[0])
+    X = torch.tensor(X0, device="cuda")
+    S = gsb.status_buffer(X0.shape[0])
+    gsb.solve_batch(X, S, prob, m, gsb.PerSystem(torch.tensor(Y, device="cuda")), options=opts,
+                    order=torch.tensor(perm, device="cuda"))
+    assert X.cpu().numpy().tobytes() == xg.tobytes()
+    assert gsb.statuses(S).tobytes() == sg.tobytes()

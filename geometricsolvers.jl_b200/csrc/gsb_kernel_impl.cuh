@@ -267,7 +267,7 @@ __global__ void __launch_bounds__(kThreads) team_kernel(const __grid_constant__ 
 // system closes stores it and takes the range's next system from a shared-memory counter. Each
 // system's solve is the same sequence of steps as a solve of its own.
 template <class Fam, bool F, bool Mixed>
-__global__ void __launch_bounds__(kThreads, 3) lm_kernel(const __grid_constant__ GsbMethod m,
+__global__ void __launch_bounds__(kThreads, 2) lm_kernel(const __grid_constant__ GsbMethod m,
                                  const __grid_constant__ GsbOptions o,
                                  const __grid_constant__ Launch L) {
     extern __shared__ double smem[];

@@ -135,14 +135,13 @@ def bytes_per_system(n):
 
 
 def measured_peaks():
+    """The HBM copy bandwidth of MEASURED_PEAKS.json (measured on this pool's B200s), else the
+    pool's earlier measurement of 6650 GB/s, with a label that says which."""
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
-    hbm = 6650.0
-    src = "fallback"
     if os.path.exists(path):
         with open(path) as fh:
-            hbm = float(json.load(fh)["hbm_gbs"])
-        src = "measured"
-    return hbm, src
+            return float(json.load(fh)["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    return 6650.0, "fallback 6650 GB/s (MEASURED_PEAKS.json absent)"
 
 
 def fp_peaks():
@@ -425,7 +424,7 @@ def main():
     if t_bytes >= t_flops:
         roof = {"bound": "hbm", "achieved": achieved_gbs, "peak": hbm_peak, "unit": "GB/s",
                 "frac": achieved_gbs / hbm_peak, "traffic": traffic,
-                "peak_source": f"{hbm_src} (MEASURED_PEAKS.json hbm_gbs)"}
+                "peak_source": hbm_src}
     else:
         roof = {"bound": "fp64", "achieved": achieved_tf, "peak": peaks["fp64"],
                 "unit": "TFLOP/s", "frac": achieved_tf / peaks["fp64"], "traffic": traffic,
@@ -619,7 +618,7 @@ def _roof(bytes_total, flops, kms, peaks, hbm_peak, hbm_src, kernel):
     tf = flops / (kms * 1e-3) / 1e12
     if t_bytes >= t_flops:
         r = {"bound": "hbm", "achieved": gbs, "peak": hbm_peak, "unit": "GB/s",
-             "frac": gbs / hbm_peak, "peak_source": f"{hbm_src} (MEASURED_PEAKS.json hbm_gbs)"}
+             "frac": gbs / hbm_peak, "peak_source": hbm_src}
     else:
         r = {"bound": "fp64", "achieved": tf, "peak": peaks["fp64"], "unit": "TFLOP/s",
              "frac": tf / peaks["fp64"], "peak_source": "measured (FP64 FMA probe, libgsbpeak)"}

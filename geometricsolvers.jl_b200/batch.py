@@ -10,6 +10,7 @@ kernel before it returns. Host checks raise before any launch, with the referenc
 
 from __future__ import annotations
 
+import contextlib
 import ctypes
 
 import numpy as np
@@ -44,6 +45,23 @@ def _check_device_f64(t, what):
         raise ArgumentError(f"{what} must be float64")
     if not t.is_contiguous():
         raise ArgumentError(f"{what} must be contiguous")
+
+
+_abi_cache = {}
+
+
+def _abi_of(obj):
+    """The C-ABI struct of a (frozen, hashable) Newton or Options, built once per distinct
+    value: the library only reads it."""
+    try:
+        return _abi_cache[obj]
+    except KeyError:
+        if len(_abi_cache) > 256:
+            _abi_cache.clear()
+        v = _abi_cache[obj] = obj.to_abi()
+        return v
+    except TypeError:  # not hashable
+        return obj.to_abi()
 
 
 def _resolve_options(options, kwargs):
@@ -157,7 +175,7 @@ def solve_batch(X, S, prob=None, method=None, p=None, *, order=None, options=Non
                 f"status vector backend {S.device} does not match batch backend {Xt.device}")
         S_buf = S
         s_kind = abi.GSB_STATUS64
-    gm = method.to_abi()
+    gm = _abi_of(method)
     if nsys == 0:
         return ReturnCodeCounts(0, 0, 0, 0, 0, 0) if counts_form else S
     lib = abi.load_library()
@@ -165,19 +183,22 @@ def solve_batch(X, S, prob=None, method=None, p=None, *, order=None, options=Non
     gp = prob.to_abi(None if sh is None else sh.data_ptr())
     if shared_A is not None:
         gp.shared, gp.shared_len = shared_A.data_ptr(), shared_A.numel()
-    go = opt.to_abi()
+    go = _abi_of(opt)
     if stream is None:
         stream = torch.cuda.current_stream(Xt.device)
-    tally = abi.GsbTally()
-    with torch.cuda.device(Xt.device):
+    tally = abi.GsbTally() if counts_form else None
+    # the launch goes to the device of X; a context switch only when it is not the current one
+    on_dev = torch.cuda.current_device() == Xt.device.index
+    with contextlib.nullcontext() if on_dev else torch.cuda.device(Xt.device):
+        st = ctypes.c_void_p(stream.cuda_stream)
         rc = lib.gsb_solve_batch(
             ctypes.byref(gp), ctypes.byref(gm), ctypes.byref(go), Xt.data_ptr(), x_layout,
             S_buf.data_ptr(), s_kind, Pt.data_ptr(), p_layout,
-            None if order_t is None else order_t.data_ptr(), 0, nsys,
-            ctypes.c_void_p(stream.cuda_stream), ctypes.byref(tally) if counts_form else None,
+            None if order_t is None else order_t.data_ptr(), 0, nsys, st,
+            ctypes.byref(tally) if counts_form else None,
         )
         _raise_for(rc, lib)
-        _raise_for(lib.gsb_synchronize(ctypes.c_void_p(stream.cuda_stream)), lib)
+        _raise_for(lib.gsb_synchronize(st), lib)
     if counts_form:
         return ReturnCodeCounts(*[int(c) for c in tally.counts])
     return S

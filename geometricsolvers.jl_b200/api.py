@@ -418,8 +418,18 @@ class NonlinearProblem:
         return p
 
     def shared_device(self, device):
-        """The family's shared constants as a float64 tensor on `device` (cached)."""
+        """The family's shared constants as a float64 tensor on `device` (cached; None for a
+        family without them)."""
         import torch
+
+        key = (device.type, device.index) if isinstance(device, torch.device) else str(device)
+        try:
+            return self._shared_dev[key]
+        except KeyError:
+            sh = self.family.shared()
+            v = None if sh is None else torch.tensor(sh, dtype=torch.float64, device=device)
+            self._shared_dev[key] = v
+            return v
 
         sh = self.family.shared()
         if sh is None:

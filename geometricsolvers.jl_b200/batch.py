@@ -150,7 +150,7 @@ def solve_batch(X, S, prob=None, method=None, p=None, *, order=None, options=Non
             f"PerSystem parameter length {plen} does not match batch length {nsys}")
     if (Pt.shape[1] if p_layout == abi.GSB_AOS else Pt.shape[0]) != npar:
         raise DimensionMismatch(f"each system takes {npar} parameters")
-    if Pt.device != Xt.device:
+    if Pt.get_device() != Xt.get_device():
         raise ArgumentError("PerSystem data must be on the device of X")
     order_t = None
     if order is not None:
@@ -170,7 +170,7 @@ def solve_batch(X, S, prob=None, method=None, p=None, *, order=None, options=Non
         if S.numel() != nsys * 72:
             raise DimensionMismatch(
                 f"status vector length {S.numel() // 72} does not match batch length {nsys}")
-        if S.device != Xt.device:
+        if S.get_device() != Xt.get_device():
             raise ArgumentError(
                 f"status vector backend {S.device} does not match batch backend {Xt.device}")
         S_buf = S

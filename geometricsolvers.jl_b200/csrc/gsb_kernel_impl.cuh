@@ -265,7 +265,8 @@ __global__ void __launch_bounds__(kThreads) team_kernel(const __grid_constant__ 
 // while the rest converge early) and a warp steps as long as its slowest lane, so the grid holds
 // the resident CTAs only, each CTA works through a contiguous range of systems, and a lane whose
 // system closes stores it and takes the range's next system from a shared-memory counter. Each
-// system's solve is the same sequence of steps as a solve of its own.
+// system's solve is the same sequence of steps as a solve of its own. Two CTAs per SM: the solve
+// then fits its registers without spilling, which measured faster than three CTAs at 168.
 template <class Fam, bool F, bool Mixed>
 __global__ void __launch_bounds__(kThreads, 2) lm_kernel(const __grid_constant__ GsbMethod m,
                                  const __grid_constant__ GsbOptions o,

@@ -50,6 +50,10 @@ def parse():
                          "65,536 systems; c2: the exponential-sum least-squares fit; c3: the "
                          "Gauss-3 stage systems with the learned warm start; c4: the "
                          "ragged batch of sizes 2..32 (one GPU)")
+    ap.add_argument("--launch-check", action="store_true",
+                    help="start the ranks as for a run and take the job's collectives (barrier, "
+                         "maximum and sum over ranks) over gloo on the CPU, rank 0 printing the "
+                         "world size: the multi-rank launcher without a GPU")
     ap.add_argument("--n", type=int, default=N_UNKNOWNS,
                     help="cubic-affine size of a --profile run (A = 6I + ... at n = 8, else (n+1)I)")
     return ap.parse_args()
@@ -229,7 +233,7 @@ class Clocks:
 # ─── the reference arm: the oracle (the CPU restatement) on the host cores ─────────────────
 
 
-def run_reference(args, rank):
+def run_reference(args, rank, world):
     if rank != 0:
         return
     import gsb200 as G
@@ -252,7 +256,7 @@ def run_reference(args, rank):
     value = sample / med
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "systems/s",
-        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": med * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Philox)",
         "config": {"workload": f"cubic-affine n=8, {args.nsys} systems, Newton+LU+Backtracking FP64",
@@ -275,14 +279,74 @@ def rel_err(x, xr):
         return np.where(den > 0, num / den, num)
 
 
+def free_port():
+    import socket
+
+    with socket.socket(socket.AF_INET, socket.SOCK_STREAM) as sk:
+        sk.bind(("127.0.0.1", 0))
+        return sk.getsockname()[1]
+
+
+def launch_ranks(args):
+    """`--gpus N` without a launcher around this process: start N ranks of the same command under
+    torch.distributed.run (one per GPU, rendezvous on 127.0.0.1) and return their exit code.
+    NCCL's initialisation log (the communicator and its rank count) goes to stderr, so stdout
+    keeps the one JSON line of rank 0."""
+    env = dict(os.environ)
+    env.setdefault("NCCL_DEBUG", "INFO")
+    env.setdefault("NCCL_DEBUG_SUBSYS", "INIT")
+    env.setdefault("NCCL_DEBUG_FILE", "/dev/stderr")
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+           f"--nproc-per-node={args.gpus}", "--master-addr", "127.0.0.1",
+           f"--master-port={free_port()}", os.path.abspath(__file__), *sys.argv[1:]]
+    proc = subprocess.Popen(cmd, env=env, start_new_session=True)
+    try:
+        return proc.wait(timeout=1800)
+    except subprocess.TimeoutExpired:
+        os.killpg(proc.pid, 9)  # the launcher's own process group: its ranks
+        proc.wait()
+        return 124
+
+
+def launch_check(rank, world):
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    if world > 1:
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=60))
+    try:
+        ranks = Ranks(world, torch.device("cpu"))
+        ranks.barrier()
+        slowest = ranks.max(float(rank))
+        count = ranks.sum(1.0)
+        ranks.barrier()
+        if rank == 0:
+            print(json.dumps({"launch_check": True, "n_gpus": world, "max_rank": slowest,
+                              "ranks_counted": count}), flush=True)
+    finally:
+        if world > 1:
+            dist.destroy_process_group()
+
+
 def main():
     args = parse()
+    if "WORLD_SIZE" not in os.environ and args.gpus > 1:
+        sys.exit(launch_ranks(args))
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    if args.impl == "reference":
-        run_reference(args, rank)
+    if world != args.gpus:
+        sys.exit(f"bench.py: --gpus {args.gpus} but the launcher started {world} ranks")
+    if args.launch_check:
+        launch_check(rank, world)
         return
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1 and (args.profile or args.workload != "c1"):
+        sys.exit("bench.py: --profile and --workload c0/c2/c3/c4 run on one GPU")
     if args.profile:
         run_profile(args)
         return

@@ -144,13 +144,21 @@ UNEVEN_SIZES = (2, 3, 4, 6, 8, 12, 16, 24, 32)
 
 
 class GsbSummary(ctypes.Structure):
+    """BatchSummary{Float64}'s layout (src/nonlinear/batched.jl:63-69): offsets 0, 8, 16, 24, 32;
+    size 40."""
+
     _fields_ = [
         ("fnorm", ctypes.c_double),
-        ("all_converged", ctypes.c_int32),
-        ("max_iterations", ctypes.c_int32),
+        ("all_converged", ctypes.c_uint8),
+        ("pad0_", ctypes.c_uint8 * 7),
         ("failure_count", ctypes.c_int64),
+        ("max_iterations", ctypes.c_int32),
+        ("pad1_", ctypes.c_int32),
         ("total_iterations", ctypes.c_int64),
     ]
+
+
+assert ctypes.sizeof(GsbSummary) == 40
 
 
 GSB_AOS, GSB_SOA = 0, 1

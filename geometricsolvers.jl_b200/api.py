@@ -418,26 +418,23 @@ class NonlinearProblem:
         return p
 
     def shared_device(self, device):
-        """The family's shared constants as a float64 tensor on `device` (cached; None for a
-        family without them)."""
+        """The family's shared constants as a float64 tensor on `device` (None for a family
+        without them). Cached per device and per value of the constants, so a family whose
+        constants change (a new step h, a new grid t) gets a fresh copy."""
         import torch
-
-        key = (device.type, device.index) if isinstance(device, torch.device) else str(device)
-        try:
-            return self._shared_dev[key]
-        except KeyError:
-            sh = self.family.shared()
-            v = None if sh is None else torch.tensor(sh, dtype=torch.float64, device=device)
-            self._shared_dev[key] = v
-            return v
 
         sh = self.family.shared()
         if sh is None:
             return None
-        key = str(device)
-        if key not in self._shared_dev:
-            self._shared_dev[key] = torch.tensor(sh, dtype=torch.float64, device=device)
-        return self._shared_dev[key]
+        sh = np.ascontiguousarray(np.asarray(sh, dtype=np.float64))
+        dkey = (device.type, device.index) if isinstance(device, torch.device) else str(device)
+        key = (dkey, sh.tobytes())
+        v = self._shared_dev.get(key)
+        if v is None:
+            if len(self._shared_dev) > 64:
+                self._shared_dev.clear()
+            v = self._shared_dev[key] = torch.tensor(sh, dtype=torch.float64, device=device)
+        return v
 
 
 class LeastSquaresProblem(NonlinearProblem):

@@ -19,13 +19,19 @@ namespace gsb {
 // Dual rules: the product of duals a*b has partials a.p b.v + b.p a.v, so with the seed
 // e_i the partial of (x_i x_i) x_i is (x_i + x_i) x_i + x_i x_i, and
 // J_ii = fma(0.1, that, A_ii).
-template <int N_, bool SharedA = false> struct CubicAffineT {
+// Rows: the block sits in a shared-memory row whose start is 16-byte aligned (the kernel stages
+// it with one bulk copy and a row stride of 2 mod 4 doubles), and A and b are read two entries
+// at a time (A(i, k), A(i+1, k) for even i), 16-byte loads that are free of bank conflicts at that
+// stride; N is even. The arithmetic is the same, row by row and in the same order.
+template <int N_, bool SharedA = false, bool Rows = false> struct CubicAffineT {
     static constexpr int N = N_, M = N_;
     // Parameters of a system: (A, b), or with SharedA (BatchParams, src/nonlinear/batched.jl:
     // 34-47) only b, A being the batch's shared block.
     static constexpr int NP = SharedA ? N_ : N_ * N_ + N_;
     static constexpr int kShared = SharedA ? N_ * N_ : 0;  // doubles of the CTA-shared block
     static constexpr bool lsq = false;
+    static constexpr bool kPairs = Rows;
+    static_assert(!Rows || (N_ % 2 == 0 && !SharedA), "paired reads: even N, a per-system A");
     const double* p;            // this system's parameter block in shared memory
     const double* a = nullptr;  // the shared A (column-major) in shared memory, with SharedA
     struct JState {
@@ -39,7 +45,35 @@ template <int N_, bool SharedA = false> struct CubicAffineT {
         return par(i + k * N);
     }
     __device__ __forceinline__ double bv(int i) const { return SharedA ? par(i) : par(N * N + i); }
+    // (A(i, k), A(i+1, k)) and (b_i, b_i+1) for even i, with Rows
+    __device__ __forceinline__ void A2(int i, int k, double& v0, double& v1) const {
+        lds2(smem_addr(p) + 8u * (i + k * N), v0, v1);
+    }
+    __device__ __forceinline__ void b2(int i, double& v0, double& v1) const {
+        lds2(smem_addr(p) + 8u * (N * N + i), v0, v1);
+    }
     __device__ __forceinline__ void F(const double (&x)[N], double (&out)[M]) const {
+        if constexpr (Rows) {
+#pragma unroll
+            for (int i = 0; i < N; i += 2) {
+                double a0, a1;
+                A2(i, 0, a0, a1);
+                double t0 = __dmul_rn(a0, x[0]), t1 = __dmul_rn(a1, x[0]);
+#pragma unroll
+                for (int j = 1; j < N; ++j) {
+                    A2(i, j, a0, a1);
+                    t0 = __fma_rn(a0, x[j], t0);
+                    t1 = __fma_rn(a1, x[j], t1);
+                }
+                const double c0 = __dmul_rn(__dmul_rn(x[i], x[i]), x[i]);
+                const double c1 = __dmul_rn(__dmul_rn(x[i + 1], x[i + 1]), x[i + 1]);
+                double b0, b1;
+                b2(i, b0, b1);
+                out[i] = __dsub_rn(__fma_rn(0.1, c0, t0), b0);
+                out[i + 1] = __dsub_rn(__fma_rn(0.1, c1, t1), b1);
+            }
+            return;
+        }
 #pragma unroll
         for (int i = 0; i < N; ++i) {
             double t = __dmul_rn(A(i, 0), x[0]);
@@ -49,33 +83,73 @@ template <int N_, bool SharedA = false> struct CubicAffineT {
             out[i] = __dsub_rn(__fma_rn(0.1, c, t), bv(i));
         }
     }
+    // A(i, i): with Rows, from the aligned pair that holds it
+    __device__ __forceinline__ double Aii(int i) const {
+        if constexpr (Rows) {
+            double v0, v1;
+            if (i % 2 == 0) {
+                A2(i, i, v0, v1);
+                return v0;
+            }
+            A2(i - 1, i, v0, v1);
+            return v1;
+        }
+        return A(i, i);
+    }
     __device__ __forceinline__ void jacobian(const double (&x)[N], JState& js) const {
 #pragma unroll
         for (int i = 0; i < N; ++i) {
             double v = x[i];
             double cp = __dadd_rn(__dmul_rn(__dadd_rn(v, v), v), __dmul_rn(v, v));
-            js.diag[i] = __fma_rn(0.1, cp, A(i, i));
+            js.diag[i] = __fma_rn(0.1, cp, Aii(i));
         }
     }
     __device__ __forceinline__ double J(const JState& js, int i, int k) const {
         return i == k ? js.diag[i] : A(i, k);
     }
+    // (J(i, k), J(i+1, k)) for even i, with Rows
+    __device__ __forceinline__ void J2(const JState& js, int i, int k, double& v0, double& v1) const {
+        A2(i, k, v0, v1);
+        if (i == k) v0 = js.diag[i];
+        if (i + 1 == k) v1 = js.diag[i + 1];
+    }
     __device__ __forceinline__ void jvp(const double (&x)[N], const double (&v)[N],
                                         double (&out)[M]) const {
+        auto rest = [&](int i, double t) {
+            double xv = __dmul_rn(v[i], x[i]);
+            double x2p = __dadd_rn(xv, xv);
+            double cp = __dadd_rn(__dmul_rn(x2p, x[i]), __dmul_rn(v[i], __dmul_rn(x[i], x[i])));
+            return __fma_rn(0.1, cp, t);
+        };
+        if constexpr (Rows) {
+#pragma unroll
+            for (int i = 0; i < N; i += 2) {
+                double a0, a1;
+                A2(i, 0, a0, a1);
+                double t0 = __dmul_rn(a0, v[0]), t1 = __dmul_rn(a1, v[0]);
+#pragma unroll
+                for (int j = 1; j < N; ++j) {
+                    A2(i, j, a0, a1);
+                    t0 = __fma_rn(a0, v[j], t0);
+                    t1 = __fma_rn(a1, v[j], t1);
+                }
+                out[i] = rest(i, t0);
+                out[i + 1] = rest(i + 1, t1);
+            }
+            return;
+        }
 #pragma unroll
         for (int i = 0; i < N; ++i) {
             double t = __dmul_rn(A(i, 0), v[0]);
 #pragma unroll
             for (int j = 1; j < N; ++j) t = __fma_rn(A(i, j), v[j], t);
-            double xv = __dmul_rn(v[i], x[i]);
-            double x2p = __dadd_rn(xv, xv);
-            double cp = __dadd_rn(__dmul_rn(x2p, x[i]), __dmul_rn(v[i], __dmul_rn(x[i], x[i])));
-            out[i] = __fma_rn(0.1, cp, t);
+            out[i] = rest(i, t);
         }
     }
 };
 template <int N> using CubicAffine = CubicAffineT<N, false>;
 template <int N> using CubicAffineSharedA = CubicAffineT<N, true>;
+template <int N> using CubicAffineRows = CubicAffineT<N, false, true>;
 
 // The shared block of a family (0 doubles for families without one).
 template <class Fam, class = void> struct SharedLen {
@@ -84,6 +158,36 @@ template <class Fam, class = void> struct SharedLen {
 template <class Fam> struct SharedLen<Fam, decltype(void(Fam::kShared))> {
     static constexpr int value = Fam::kShared;
 };
+
+// Whether a family reads its block in aligned pairs (and needs 16-byte aligned rows).
+template <class Fam, class = void> struct PairsOf {
+    static constexpr bool value = false;
+};
+template <class Fam> struct PairsOf<Fam, decltype(void(Fam::kPairs))> {
+    static constexpr bool value = Fam::kPairs;
+};
+
+// Every entry of a family's Jacobian, column by column and down each column (the order of the
+// factor's load and of grad_ratio_and_norm's sums): body(i, k, J(i, k)). A family with aligned
+// pairs reads (J(i, k), J(i+1, k)) at once.
+template <class Fam, class Body>
+__device__ __forceinline__ void for_each_J(const Fam& fam, const typename Fam::JState& js, Body body) {
+#pragma unroll
+    for (int k = 0; k < Fam::N; ++k) {
+        if constexpr (PairsOf<Fam>::value) {
+#pragma unroll
+            for (int i = 0; i < Fam::M; i += 2) {
+                double v0, v1;
+                fam.J2(js, i, k, v0, v1);
+                body(i, k, v0);
+                body(i + 1, k, v1);
+            }
+        } else {
+#pragma unroll
+            for (int i = 0; i < Fam::M; ++i) body(i, k, fam.J(js, i, k));
+        }
+    }
+}
 
 // A family with an analytic Jacobian (the problem's `J`, src/ad/forwarddiff_static.jl:36-38)
 // holds the full matrix; its JVP is J(x) v as a left fold (src/ad/jvp.jl:88-91).

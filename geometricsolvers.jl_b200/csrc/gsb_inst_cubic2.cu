@@ -2,5 +2,5 @@
 #include "gsb_kernel_impl.cuh"
 
 namespace gsb {
-GSB_DEFINE_ENTRY(cubic2, CubicAffine<2>)
+GSB_DEFINE_ENTRY(cubic2, CubicAffineRows<2>)
 }  // namespace gsb

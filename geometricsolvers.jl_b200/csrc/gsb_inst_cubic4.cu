@@ -2,5 +2,5 @@
 #include "gsb_kernel_impl.cuh"
 
 namespace gsb {
-GSB_DEFINE_ENTRY(cubic4, CubicAffine<4>)
+GSB_DEFINE_ENTRY(cubic4, CubicAffineRows<4>)
 }  // namespace gsb

@@ -2,5 +2,5 @@
 #include "gsb_kernel_impl.cuh"
 
 namespace gsb {
-GSB_DEFINE_ENTRY(cubic6, CubicAffine<6>)
+GSB_DEFINE_ENTRY(cubic6, CubicAffineRows<6>)
 }  // namespace gsb

@@ -2,5 +2,5 @@
 #include "gsb_kernel_impl.cuh"
 
 namespace gsb {
-GSB_DEFINE_ENTRY(cubic8, CubicAffine<8>)
+GSB_DEFINE_ENTRY(cubic8, CubicAffineRows<8>)
 }  // namespace gsb

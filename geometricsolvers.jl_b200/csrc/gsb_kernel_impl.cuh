@@ -11,6 +11,7 @@
 #include "gsb_newton.cuh"
 #include "gsb_numerics.cuh"
 #include "gsb_team.cuh"
+#include "gsb_umma.cuh"
 #include "gsb_warp.cuh"
 
 namespace gsb {
@@ -41,6 +42,9 @@ struct Launch {
     // the launch; the launch then solves order[first .. first + count) instead of order[0 ..
     // nsys). nullptr otherwise.
     const unsigned long long* bucket;
+    // Set to nonzero when a wait for a staging copy ran out (the systems of that CTA are then
+    // left unsolved); nullptr for none.
+    unsigned* fault;
 };
 
 // The systems a launch solves: `n` entries of `order` (or 0 .. n-1 without one).
@@ -89,6 +93,56 @@ __device__ __forceinline__ double* x_block(const Launch& L, int64_t idx, int n) 
 // of each half-warp access.
 __host__ __device__ constexpr int row_stride(int np, int n) {
     return ((np + 2 * n) % 2 == 1) ? np + 2 * n : np + 2 * n + 1;
+}
+
+// The row stride of the one-thread kernel. A family that reads its block in aligned pairs
+// (PairsOf) takes 16-byte aligned rows, staged by one bulk copy each: a stride of 2 mod 4
+// doubles, at which the 16-byte accesses of each quarter-warp fall on distinct banks.
+template <class Fam> __host__ __device__ constexpr int newton_row_stride() {
+    if constexpr (PairsOf<Fam>::value) {
+        constexpr int need = Fam::NP + 2 * Fam::N;
+        return need + ((2 - need % 4) + 4) % 4;
+    } else {
+        return row_stride(Fam::NP, Fam::N);
+    }
+}
+
+// Polls of a staging wait before it gives up: far beyond the microseconds a copy of a few hundred
+// bytes takes, and finite.
+constexpr uint32_t kStageWaitPolls = 1u << 22;
+
+// Stage one system's parameter block (NP doubles from src) into a 16-byte aligned shared row by
+// one bulk copy that completes on `bar` (the thread arrives with the bytes it expects), or, when
+// the source is not 16-byte aligned, by loads and stores of its own followed by a plain arrival.
+template <int NP>
+__device__ __forceinline__ void stage_row_bulk(double* row, const double* src, uint64_t* bar) {
+    static_assert((NP * 8) % 16 == 0, "a bulk copy moves a multiple of 16 bytes");
+    const unsigned b = smem_addr(bar);
+    if ((reinterpret_cast<uintptr_t>(src) & 15u) == 0) {
+        umma::fence_async_shared();  // earlier generic accesses of the row before the copy's writes
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"(NP * 8)
+                     : "memory");
+        asm volatile(
+            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                smem_addr(row)),
+            "l"(src), "r"(NP * 8), "r"(b)
+            : "memory");
+        return;
+    }
+#pragma unroll 4
+    for (int k = 0; k < NP; ++k) row[k] = __ldg(src + k);
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(b) : "memory");
+}
+// A system's start iterate into registers (AoS, SoA, or ragged offsets).
+template <int N>
+__device__ __forceinline__ void load_x(const Launch& L, int64_t idx, double (&x)[N]) {
+    const double* xb = x_block(L, idx, N);
+#pragma unroll
+    for (int k = 0; k < N; ++k) x[k] = L.x_layout == GSB_SOA ? L.X[(int64_t)k * L.nsys + idx] : xb[k];
+}
+
+__device__ __forceinline__ void stage_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
 }
 
 __device__ __forceinline__ void store_status(void* S, int64_t idx, const DevStatus& s, double gr) {
@@ -160,19 +214,57 @@ template <class Fam, bool F, bool Mixed, bool PlainRef, bool Persistent, bool Qr
 __global__ void __launch_bounds__(kThreads, (min_blocks<Fam, Mixed>())) newton_kernel(const __grid_constant__ GsbMethod m,
                                  const __grid_constant__ GsbOptions o,
                                  const __grid_constant__ Launch L) {
-    extern __shared__ double smem[];
-    constexpr int N = Fam::N, NP = Fam::NP, RS = row_stride(NP, N);
+    extern __shared__ __align__(16) double smem[];
+    constexpr int N = Fam::N, NP = Fam::NP, RS = newton_row_stride<Fam>();
+    constexpr bool kBulk = PairsOf<Fam>::value;
     // a family's block shared by the batch (BatchParams) first, then one row per thread
     constexpr int SH = SharedLen<Fam>::value, SHP = ((SH + 1) / 2) * 2;
     const int tid = threadIdx.x;
     double* rows = smem + SHP;
     double* prow = rows + tid * RS;
+    __shared__ __align__(8) uint64_t bar;  // completion of a chunk's row copies (kBulk)
+    uint32_t phase = 0;
     if constexpr (SH > 0) {
         for (int q = tid; q < SH; q += kThreads) smem[q] = __ldg(L.shared + q);
     }
+    if constexpr (kBulk) {
+        if (tid == 0) {
+            umma::mbar_init(&bar, kThreads);
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        }
+        __syncthreads();
+    }
     for_each_chunk<Persistent>(L, kThreads, [&](int64_t base, const Range& r) {
         const int64_t i = base + tid;
-        if (r.order == nullptr && L.p_layout == GSB_AOS && L.p_off == nullptr) {
+        double x[N];
+        if constexpr (kBulk) {
+            // every thread stages its own system's row and arrives; the CTA waits for all,
+            // with the thread's iterate loads in flight meanwhile
+            if (i < r.n) {
+                const int64_t idx = r.order ? r.order[i] - L.order_base : i;
+                if (L.p_layout == GSB_SOA) {
+#pragma unroll 4
+                    for (int k = 0; k < NP; ++k) prow[k] = __ldg(L.P + (int64_t)k * L.nsys + idx);
+                    stage_arrive(&bar);
+                } else {
+                    stage_row_bulk<NP>(prow, param_block(L, idx, NP), &bar);
+                }
+            } else {
+                stage_arrive(&bar);
+            }
+            if (i < r.n) load_x<N>(L, r.order ? r.order[i] - L.order_base : i, x);
+            // the barrier that also publishes the rows stored by threads themselves; every
+            // thread learns whether all copies landed
+            const bool staged = __syncthreads_and(umma::mbar_wait(&bar, phase, kStageWaitPolls));
+            phase ^= 1u;
+            if (!staged) {
+                // the copies did not land: record it, give them a second bounded wait, and
+                // leave this CTA's systems unsolved
+                if (L.fault && tid == 0) *reinterpret_cast<volatile unsigned*>(L.fault) = 1u;
+                umma::mbar_wait(&bar, phase ^ 1u, kStageWaitPolls);
+                return;
+            }
+        } else if (r.order == nullptr && L.p_layout == GSB_AOS && L.p_off == nullptr) {
             stage_aos<NP, RS, kThreads>(rows, L.P + base * NP, r.n - base, tid);
         } else if (i < r.n) {
             const int64_t idx = r.order ? r.order[i] - L.order_base : i;
@@ -185,16 +277,13 @@ __global__ void __launch_bounds__(kThreads, (min_blocks<Fam, Mixed>())) newton_k
                 for (int k = 0; k < NP; ++k) prow[k] = __ldg(pb + k);
             }
         }
-        __syncthreads();
+        if constexpr (!kBulk) __syncthreads();
         if (i >= r.n) return;
         const int64_t idx = r.order ? r.order[i] - L.order_base : i;
         Fam fam{prow};
         if constexpr (SH > 0) fam.a = smem;
-        double x[N];
         double* xb = x_block(L, idx, N);
-#pragma unroll
-        for (int k = 0; k < N; ++k)
-            x[k] = L.x_layout == GSB_SOA ? L.X[(int64_t)k * L.nsys + idx] : xb[k];
+        if constexpr (!kBulk) load_x<N>(L, idx, x);
         Solver<Fam, F, Mixed, PlainRef, Qr> sv(fam, m, o, N >= 6 ? prow + NP : nullptr);
         double gr;
         DevStatus s = sv.solve(x, gr);
@@ -407,7 +496,7 @@ struct KernelEntry {
 template <class Fam, bool F, bool Mixed, bool PlainRef> KernelEntry* entry() {
     static KernelEntry e{newton_kernel<Fam, F, Mixed, PlainRef, false>,
                          newton_kernel<Fam, F, Mixed, PlainRef, true>,
-                         ((SharedLen<Fam>::value + 1) / 2) * 2 + kThreads * row_stride(Fam::NP, Fam::N),
+                         ((SharedLen<Fam>::value + 1) / 2) * 2 + kThreads * newton_row_stride<Fam>(),
                          kThreads, {}};
     return &e;
 }
@@ -416,7 +505,7 @@ template <class Fam, bool F, bool Mixed, bool PlainRef> KernelEntry* entry() {
 template <class Fam, bool F> KernelEntry* qr_entry() {
     static KernelEntry e{newton_kernel<Fam, F, false, false, false, true>,
                          newton_kernel<Fam, F, false, false, true, true>,
-                         ((SharedLen<Fam>::value + 1) / 2) * 2 + kThreads * row_stride(Fam::NP, Fam::N),
+                         ((SharedLen<Fam>::value + 1) / 2) * 2 + kThreads * newton_row_stride<Fam>(),
                          kThreads, {}};
     return &e;
 }

@@ -111,6 +111,18 @@ __global__ void noalloc_check_order(const int64_t* order, int order_base, int64_
 
 using namespace gsb;
 
+// The structs that cross the boundary have the layouts of the reference's types.
+#include <cstddef>
+static_assert(sizeof(GsbStatus64) == 72 && offsetof(GsbStatus64, fnorm) == 8 &&
+                  offsetof(GsbStatus64, step_failures) == 24 && offsetof(GsbStatus64, rank) == 32 &&
+                  offsetof(GsbStatus64, gradratio) == 48 && offsetof(GsbStatus64, reused) == 65,
+              "GsbStatus64 is SolverStatus{Float64}");
+static_assert(sizeof(GsbSummary) == 40 && offsetof(GsbSummary, all_converged) == 8 &&
+                  offsetof(GsbSummary, failure_count) == 16 &&
+                  offsetof(GsbSummary, max_iterations) == 24 &&
+                  offsetof(GsbSummary, total_iterations) == 32,
+              "GsbSummary is BatchSummary{Float64}");
+
 // ─── host side ──────────────────────────────────────────────────────────────────────────────
 
 namespace {
@@ -147,6 +159,40 @@ int workspace(Workspace** out) {
         if (int rc = cuda_err(cudaMalloc(&w.acc, sizeof(SummaryAcc)), "cudaMalloc")) return rc;
     }
     *out = &w;
+    return 0;
+}
+
+// A word of mapped pinned host memory that a batch kernel sets when one of its staging waits
+// ran out (its systems then stay unsolved): allocated once per process, read by the host after a
+// synchronisation without a copy. nullptr when the allocation failed (no word is then set).
+std::mutex g_fault_mu;
+unsigned* g_fault = nullptr;
+bool g_fault_tried = false;
+
+unsigned* fault_word() {
+    std::lock_guard<std::mutex> lk(g_fault_mu);
+    if (!g_fault_tried) {
+        g_fault_tried = true;
+        void* h = nullptr;
+        if (cudaHostAlloc(&h, sizeof(unsigned), cudaHostAllocMapped | cudaHostAllocPortable) ==
+            cudaSuccess) {
+            *static_cast<volatile unsigned*>(h) = 0u;
+            g_fault = static_cast<unsigned*>(h);
+        } else {
+            cudaGetLastError();  // the failed allocation's error is not the caller's
+        }
+    }
+    return g_fault;
+}
+
+// After a synchronisation: an error if a kernel reported a staging wait that ran out.
+int check_fault() {
+    if (g_fault && *reinterpret_cast<volatile unsigned*>(g_fault) != 0u) {
+        *reinterpret_cast<volatile unsigned*>(g_fault) = 0u;
+        return set_err(GSB_ERR_CUDA,
+                       "a batch kernel's wait for its staging copies ran out; systems of that "
+                       "launch were left unsolved");
+    }
     return 0;
 }
 
@@ -423,7 +469,7 @@ int launch_blocks(const KernelEntry* ke, int64_t nsys, size_t smem, int64_t* blo
 int launch_solve(const GsbProblem* prob, const GsbMethod* method, const GsbOptions* opt, double* X,
                  int32_t x_layout, void* S, int32_t s_kind, const double* P, int32_t p_layout,
                  const int64_t* order, int32_t order_base, int64_t nsys, cudaStream_t st,
-                 unsigned long long* tally_dev) {
+                 unsigned long long* tally_dev, unsigned* fault) {
     KernelEntry* ke = nullptr;
     if (int rc = select_entry(prob, method, &ke)) return rc;
     int dev = 0;
@@ -438,6 +484,7 @@ int launch_solve(const GsbProblem* prob, const GsbMethod* method, const GsbOptio
         ke->attr_set[dev & 63] = true;
     }
     Launch L{X, x_layout, S, s_kind, P, p_layout, order, order_base, nsys, prob->shared, tally_dev};
+    L.fault = fault;
     int64_t blocks = 0;
     if (int rc = launch_blocks(ke, nsys, smem, &blocks)) return rc;
     ke->fn<<<(unsigned)blocks, kThreads, smem, st>>>(*method, *opt, L);
@@ -566,6 +613,7 @@ int gsb_solve_batch(const GsbProblem* prob, const GsbMethod* method, const GsbOp
     }
     Launch L{X, x_layout, S, s_kind, P, p_layout, order, order_base, nsys, prob->shared,
              ws ? ws->tally : nullptr};
+    L.fault = fault_word();
     int64_t blocks = 0;
     if (int rc = launch_blocks(ke, nsys, smem, &blocks)) return rc;
     ke->fn<<<(unsigned)blocks, kThreads, smem, st>>>(*method, *opt, L);
@@ -576,6 +624,7 @@ int gsb_solve_batch(const GsbProblem* prob, const GsbMethod* method, const GsbOp
                               "tally copy"))
             return rc;
         if (int rc = cuda_err(cudaStreamSynchronize(st), "tally copy")) return rc;
+        if (int rc = check_fault()) return rc;
         for (int c = 0; c < 6; ++c) tally->counts[c] = (int64_t)h[c];
     }
     return 0;
@@ -636,8 +685,10 @@ int gsb_batch_summary(const GsbStatus64* S, int64_t nsys, void* stream, GsbSumma
 }
 
 int gsb_synchronize(void* stream) {
-    return cuda_err(cudaStreamSynchronize(reinterpret_cast<cudaStream_t>(stream)),
-                    "cudaStreamSynchronize");
+    if (int rc = cuda_err(cudaStreamSynchronize(reinterpret_cast<cudaStream_t>(stream)),
+                          "cudaStreamSynchronize"))
+        return rc;
+    return check_fault();
 }
 
 
@@ -676,14 +727,19 @@ int gsb_solve_batch_counts_noalloc(const GsbProblem* prob, const GsbMethod* meth
         if (int rc = cuda_err(cudaStreamSynchronize(st), "flag copy")) return rc;
         if (flags) return set_err(GSB_ERR_ARGUMENT, "order is not a permutation of the batch");
     }
+    // word 7 of the array is the kernel's staging-fault word
     if (int rc = launch_solve(prob, method, opt, X, x_layout, codes, GSB_CODES, P, p_layout, order,
-                              order_base, nsys, st, scratch))
+                              order_base, nsys, st, scratch, reinterpret_cast<unsigned*>(scratch + 7)))
         return rc;
-    unsigned long long h[6];
+    unsigned long long h[8];
     if (int rc = cuda_err(cudaMemcpyAsync(h, scratch, sizeof(h), cudaMemcpyDeviceToHost, st),
                           "tally copy"))
         return rc;
     if (int rc = cuda_err(cudaStreamSynchronize(st), "tally copy")) return rc;
+    if (h[7] != 0)
+        return set_err(GSB_ERR_CUDA,
+                       "the batch kernel's wait for its staging copies ran out; systems were left "
+                       "unsolved");
     for (int c = 0; c < 6; ++c) tally->counts[c] = (int64_t)h[c];
     return 0;
 }
@@ -870,6 +926,7 @@ int uneven_capture(UnevenPlan& p, const UnevenKey& k, bool want_tally) {
         p.exec = nullptr;
     }
     const unsigned cgrid = (unsigned)std::min<int64_t>((k.nsys + 255) / 256, (int64_t)sms * 8);
+    unsigned* fault = fault_word();  // allocated (once) before the capture begins
     cudaGraph_t g = nullptr;
     if (int rc = cuda_err(cudaStreamBeginCapture(p.cs, cudaStreamCaptureModeThreadLocal), "capture"))
         return rc;
@@ -883,7 +940,7 @@ int uneven_capture(UnevenPlan& p, const UnevenKey& k, bool want_tally) {
         cudaStreamWaitEvent(p.side[b], p.fork, 0);
         Launch L{k.X, GSB_AOS, k.S, k.s_kind, k.P, GSB_AOS, p.list, 0, k.nsys, nullptr,
                  want_tally ? p.work->tally : nullptr, k.x_off, k.p_off, &p.work->queue[b],
-                 &p.work->range[b][0]};
+                 &p.work->range[b][0], fault};
         ke[b]->fn_persistent<<<grid[b], kThreads, (size_t)ke[b]->smem_doubles * sizeof(double), p.side[b]>>>(
             k.m, k.o, L);
         cudaEventRecord(p.join[b], p.side[b]);
@@ -965,6 +1022,7 @@ int gsb_solve_batch_uneven(const GsbMethod* method, const GsbOptions* opt, doubl
                           "tally copy"))
         return rc;
     if (int rc = cuda_err(cudaStreamSynchronize(st), "synchronize")) return rc;
+    if (int rc = check_fault()) return rc;
     if (tally)
         for (int c = 0; c < 6; ++c) tally->counts[c] = (int64_t)h[1 + c];
     if (h[0]) return set_err(GSB_ERR_ARGUMENT, std::to_string(h[0]) +
@@ -1065,33 +1123,57 @@ int gsb_solve_batch_host(const GsbProblem* prob, const GsbMethod* method, const 
     if (int rc = pipe_setup(hp, chunk * n * 8, chunk * np * 8, chunk * sbytes)) return rc;
     if (int rc = cuda_err(cudaMemsetAsync(hp.tally, 0, 6 * sizeof(unsigned long long), hp.comp), "memset"))
         return rc;
+    // Every call's return code is checked. On an error after the first copy is queued, the three
+    // streams are drained before returning, so that no copy still writes into X or S (or reads
+    // the staging slots of a next call) once the caller has been told the call failed.
+    auto drain = [&](int rc) {
+        cudaStreamSynchronize(hp.h2d);
+        cudaStreamSynchronize(hp.comp);
+        cudaStreamSynchronize(hp.d2h);
+        cudaGetLastError();
+        return rc;
+    };
     const int64_t nchunks = (nsys + chunk - 1) / chunk;
+    unsigned* fault = fault_word();
     for (int64_t c = 0; c < nchunks; ++c) {
         const int k = (int)(c % kSlots);
         const int64_t first = c * chunk;
         const int64_t len = std::min(chunk, nsys - first);
         // the slot's previous results have left before its new inputs arrive
-        if (c >= kSlots) cudaStreamWaitEvent(hp.h2d, hp.out[k], 0);
-        cudaMemcpyAsync(hp.x[k], X + first * n, len * n * 8, cudaMemcpyHostToDevice, hp.h2d);
-        cudaMemcpyAsync(hp.p[k], P + first * np, len * np * 8, cudaMemcpyHostToDevice, hp.h2d);
-        cudaEventRecord(hp.in[k], hp.h2d);
-        cudaStreamWaitEvent(hp.comp, hp.in[k], 0);
+        if (c >= kSlots)
+            if (int rc = cuda_err(cudaStreamWaitEvent(hp.h2d, hp.out[k], 0), "wait")) return drain(rc);
+        if (int rc = cuda_err(cudaMemcpyAsync(hp.x[k], X + first * n, len * n * 8,
+                                              cudaMemcpyHostToDevice, hp.h2d), "copy in"))
+            return drain(rc);
+        if (int rc = cuda_err(cudaMemcpyAsync(hp.p[k], P + first * np, len * np * 8,
+                                              cudaMemcpyHostToDevice, hp.h2d), "copy in"))
+            return drain(rc);
+        if (int rc = cuda_err(cudaEventRecord(hp.in[k], hp.h2d), "event")) return drain(rc);
+        if (int rc = cuda_err(cudaStreamWaitEvent(hp.comp, hp.in[k], 0), "wait")) return drain(rc);
         if (int rc = launch_solve(prob, method, opt, hp.x[k], GSB_AOS, hp.s[k], s_kind, hp.p[k],
-                                  GSB_AOS, nullptr, 0, len, hp.comp, tally ? hp.tally : nullptr))
-            return rc;
-        cudaEventRecord(hp.solved[k], hp.comp);
-        cudaStreamWaitEvent(hp.d2h, hp.solved[k], 0);
-        cudaMemcpyAsync(X + first * n, hp.x[k], len * n * 8, cudaMemcpyDeviceToHost, hp.d2h);
-        cudaMemcpyAsync(static_cast<unsigned char*>(S) + first * sbytes, hp.s[k], len * sbytes,
-                        cudaMemcpyDeviceToHost, hp.d2h);
-        cudaEventRecord(hp.out[k], hp.d2h);
+                                  GSB_AOS, nullptr, 0, len, hp.comp, tally ? hp.tally : nullptr, fault))
+            return drain(rc);
+        if (int rc = cuda_err(cudaEventRecord(hp.solved[k], hp.comp), "event")) return drain(rc);
+        if (int rc = cuda_err(cudaStreamWaitEvent(hp.d2h, hp.solved[k], 0), "wait")) return drain(rc);
+        if (int rc = cuda_err(cudaMemcpyAsync(X + first * n, hp.x[k], len * n * 8,
+                                              cudaMemcpyDeviceToHost, hp.d2h), "copy out"))
+            return drain(rc);
+        if (int rc = cuda_err(cudaMemcpyAsync(static_cast<unsigned char*>(S) + first * sbytes,
+                                              hp.s[k], len * sbytes, cudaMemcpyDeviceToHost, hp.d2h),
+                              "copy out"))
+            return drain(rc);
+        if (int rc = cuda_err(cudaEventRecord(hp.out[k], hp.d2h), "event")) return drain(rc);
     }
     unsigned long long h[6] = {};
-    if (tally) cudaMemcpyAsync(h, hp.tally, sizeof(h), cudaMemcpyDeviceToHost, hp.comp);
+    if (tally)
+        if (int rc = cuda_err(cudaMemcpyAsync(h, hp.tally, sizeof(h), cudaMemcpyDeviceToHost, hp.comp),
+                              "tally copy"))
+            return drain(rc);
     cudaError_t e = cudaStreamSynchronize(hp.comp);
     if (e == cudaSuccess) e = cudaStreamSynchronize(hp.d2h);
     if (e == cudaSuccess) e = cudaStreamSynchronize(hp.h2d);
-    if (int rc = cuda_err(e, "host batch")) return rc;
+    if (int rc = cuda_err(e, "host batch")) return drain(rc);
+    if (int rc = check_fault()) return rc;
     if (tally)
         for (int c = 0; c < 6; ++c) tally->counts[c] = (int64_t)h[c];
     return 0;

@@ -96,26 +96,28 @@ template <bool F, int N, class TF> struct LUFactor {
     __device__ __forceinline__ void load(const Fam& fam, const JS& js, const double (&Fx)[M],
                                          double& s, double (&g)[N]) {
         static_assert(sizeof(TF) == sizeof(double) && M == N, "the square Float64 factor");
-#pragma unroll
-        for (int k = 0; k < N; ++k)
-#pragma unroll
-            for (int i = 0; i < N; ++i) {
-                const double v = fam.J(js, i, k);
-                a[i + k * N] = v;
-                s = (i == 0 && k == 0) ? Arith<F>::mul(v, v) : Arith<F>::madd(v, v, s);
-                g[k] = i == 0 ? Arith<F>::mul(v, Fx[0]) : Arith<F>::madd(v, Fx[i], g[k]);
-            }
+        for_each_J(fam, js, [&](int i, int k, double v) {
+            a[i + k * N] = v;
+            s = (i == 0 && k == 0) ? Arith<F>::mul(v, v) : Arith<F>::madd(v, v, s);
+            g[k] = i == 0 ? Arith<F>::mul(v, Fx[0]) : Arith<F>::madd(v, Fx[i], g[k]);
+        });
     }
 
-    // factor_matrix's scaling of the loaded J (J / 2^e in place), then the elimination.
+    // factor_matrix's scaling of the loaded J (J / 2^e in place), then the elimination. The
+    // same-type scaling divides only for e < 0, that is when every |J_ik| < 1 (or the largest
+    // is subnormal); an entry with |J_00| >= 1 settles e = 0 without the scan of all N^2.
     __device__ __forceinline__ void eliminate() {
         static_assert(sizeof(TF) == sizeof(double), "the Float64 factor");
-        e = matrix_exponent<N * N>(a);
-        if (e < 0) {
-#pragma unroll
-            for (int q = 0; q < N * N; ++q) a[q] = scale2_in(a[q], -e);  // -e in [1, 1023]
-        } else {
+        if (fabs(a[0]) >= 1.0) {
             e = 0;
+        } else {
+            e = matrix_exponent<N * N>(a);
+            if (e < 0) {
+#pragma unroll
+                for (int q = 0; q < N * N; ++q) a[q] = scale2_in(a[q], -e);  // -e in [1, 1023]
+            } else {
+                e = 0;
+            }
         }
         elimination();
     }
@@ -125,30 +127,20 @@ template <bool F, int N, class TF> struct LUFactor {
         // J into the factor's registers, then J / 2^e in place (factor_matrix)
         constexpr bool same = sizeof(TF) == sizeof(double);
         if constexpr (same) {
-#pragma unroll
-            for (int k = 0; k < N; ++k)
-#pragma unroll
-                for (int i = 0; i < N; ++i) a[i + k * N] = fam.J(js, i, k);
+            for_each_J(fam, js, [&](int i, int k, double v) { a[i + k * N] = v; });
             eliminate();
             return;
         } else {
             unsigned long long mb = 0;
-#pragma unroll
-            for (int k = 0; k < N; ++k)
-#pragma unroll
-                for (int i = 0; i < N; ++i) {
-                    unsigned long long b = FBits<double>::bits(fam.J(js, i, k)) & ~FBits<double>::sign_mask;
-                    mb = b > mb ? b : mb;
-                }
+            for_each_J(fam, js, [&](int, int, double v) {
+                const unsigned long long b = FBits<double>::bits(v) & ~FBits<double>::sign_mask;
+                mb = b > mb ? b : mb;
+            });
             double mm = FBits<double>::from(mb);
             e = (isfin(mm) && mm != 0.0) ? max(-1023, min(1023, jexponent(mm))) : 0;
-#pragma unroll
-            for (int k = 0; k < N; ++k)
-#pragma unroll
-                for (int i = 0; i < N; ++i) {
-                    double v = fam.J(js, i, k);
-                    a[i + k * N] = TF(e == 0 ? v : scale2_in(v, -e));  // -e in [-1023, 1023]
-                }
+            for_each_J(fam, js, [&](int i, int k, double v) {
+                a[i + k * N] = TF(e == 0 ? v : scale2_in(v, -e));  // -e in [-1023, 1023]
+            });
         }
         elimination();
     }
@@ -159,13 +151,22 @@ template <bool F, int N, class TF> struct LUFactor {
 #pragma unroll
         for (int k = 0; k < N; ++k) {
             int p = k;
-            TF amax = fabs(a[k + k * N]);
+            // The pivot is the first largest |a_ik|, i >= k. When every entry below the
+            // diagonal has a smaller magnitude key (the high word with the sign shifted out,
+            // an integer order of |x|; NaN above every finite value) than a_kk, the diagonal
+            // is that pivot; the search of compares runs only otherwise.
+            unsigned below = 0;
 #pragma unroll
-            for (int i = k + 1; i < N; ++i) {
-                TF v = fabs(a[i + k * N]);
-                if (v > amax) {
-                    amax = v;
-                    p = i;
+            for (int i = k + 1; i < N; ++i) below = max(below, mag_key(a[i + k * N]));
+            if (k + 1 < N && !(below < mag_key(a[k + k * N]))) {
+                TF amax = fabs(a[k + k * N]);
+#pragma unroll
+                for (int i = k + 1; i < N; ++i) {
+                    TF v = fabs(a[i + k * N]);
+                    if (v > amax) {
+                        amax = v;
+                        p = i;
+                    }
                 }
             }
             ipiv[k] = p;
@@ -179,9 +180,9 @@ template <bool F, int N, class TF> struct LUFactor {
             if (akk == TF(0)) {
                 if (info == 0) info = k + 1;
             } else if constexpr (kRecip) {
-                // the fused Float32 factor: one reciprocal per pivot, kept in place of the
-                // pivot for the back substitution
-                const TF r = TF(1) / akk;
+                // the fused factor: one reciprocal per pivot (correctly rounded, the bits of
+                // 1 / akk), kept in place of the pivot for the back substitution
+                const TF r = crcp(akk);
                 a[k + k * N] = r;
 #pragma unroll
                 for (int i = k + 1; i < N; ++i) a[i + k * N] = a[i + k * N] * r;
@@ -230,6 +231,16 @@ template <bool F, int N, class TF> struct LUFactor {
     // ldiv!!: same type (factors.jl:931-936) or mixed type (factors.jl:943-949).
     __device__ __forceinline__ void ldiv(const double (&r)[N], double (&d)[N]) const {
         if constexpr (sizeof(TF) == sizeof(double)) {
+            if (e == 0 && rhs_unscaled<N>(r)) {
+                // rhs_exponent is 0 and so is e: no scaling on either side of the solve
+                TF x[N];
+#pragma unroll
+                for (int i = 0; i < N; ++i) x[i] = r[i];
+                backsolve(x);
+#pragma unroll
+                for (int i = 0; i < N; ++i) d[i] = x[i];
+                return;
+            }
             int k = rhs_exponent<N>(r, e);
             TF x[N];
 #pragma unroll
@@ -285,22 +296,15 @@ template <bool F, int N> struct QRFactor {
     __device__ __forceinline__ void load(const Fam& fam, const JS& js, const double (&Fx)[M],
                                          double& s, double (&g)[N]) {
         static_assert(M == N, "the square factor");
-#pragma unroll
-        for (int k = 0; k < N; ++k)
-#pragma unroll
-            for (int i = 0; i < N; ++i) {
-                const double v = fam.J(js, i, k);
-                a[i + k * N] = v;
-                s = (i == 0 && k == 0) ? A_::mul(v, v) : A_::madd(v, v, s);
-                g[k] = i == 0 ? A_::mul(v, Fx[0]) : A_::madd(v, Fx[i], g[k]);
-            }
+        for_each_J(fam, js, [&](int i, int k, double v) {
+            a[i + k * N] = v;
+            s = (i == 0 && k == 0) ? A_::mul(v, v) : A_::madd(v, v, s);
+            g[k] = i == 0 ? A_::mul(v, Fx[0]) : A_::madd(v, Fx[i], g[k]);
+        });
     }
 
     template <class Fam, class JS> __device__ __forceinline__ void factor(const Fam& fam, const JS& js) {
-#pragma unroll
-        for (int k = 0; k < N; ++k)
-#pragma unroll
-            for (int i = 0; i < N; ++i) a[i + k * N] = fam.J(js, i, k);
+        for_each_J(fam, js, [&](int i, int k, double v) { a[i + k * N] = v; });
         eliminate();
     }
 
@@ -383,6 +387,85 @@ template <bool F, int N> struct QRFactor {
         int e2 = k - e;
 #pragma unroll
         for (int i = 0; i < N; ++i) d[i] = e2 == 0 ? x[i] : scale2_in(x[i], e2);  // e2 in [0, 1029]
+    }
+};
+
+// The Float64 LU of the plain step in registers, for the common case in which it needs neither
+// a row exchange nor factor_matrix's scaling: every pivot is the diagonal (each a_kk's magnitude
+// key above those of the entries below it, as LUFactor's search decides) and |J_00| >= 1 (so
+// e = 0). factor() returns false as soon as either fails; the caller then factors with LocalLU,
+// whose operations are LUFactor's, so the results are the same bits either way. Without the
+// exchange and scaling code the elimination is one straight run of arithmetic, and the
+// back substitution takes no permutation.
+template <bool F, int N> struct DiagLU {
+    double a[N * N];
+
+    template <class Fam, class JS>
+    __device__ __forceinline__ bool factor(const Fam& fam, const JS& js) {
+        for_each_J(fam, js, [&](int i, int k, double v) { a[i + k * N] = v; });
+        if (!(fabs(a[0]) >= 1.0)) return false;  // factor_matrix might scale
+#pragma unroll
+        for (int k = 0; k < N; ++k) {
+            if (k + 1 < N) {
+                unsigned below = 0;
+#pragma unroll
+                for (int i = k + 1; i < N; ++i) below = max(below, mag_key(a[i + k * N]));
+                if (!(below < mag_key(a[k + k * N]))) return false;  // a row exchange might be due
+            } else if (a[k + k * N] == 0.0) {
+                return false;  // singular: LocalLU reports it
+            }
+            if constexpr (F) {
+                const double r = crcp(a[k + k * N]);
+                a[k + k * N] = r;
+#pragma unroll
+                for (int i = k + 1; i < N; ++i) a[i + k * N] = a[i + k * N] * r;
+            } else {
+                const double akk = a[k + k * N];
+#pragma unroll
+                for (int i = k + 1; i < N; ++i) a[i + k * N] = a[i + k * N] / akk;
+            }
+#pragma unroll
+            for (int j = k + 1; j < N; ++j)
+#pragma unroll
+                for (int i = k + 1; i < N; ++i)
+                    a[i + j * N] = Arith<F>::msub(a[i + k * N], a[k + j * N], a[i + j * N]);
+        }
+        return true;
+    }
+
+    __device__ __forceinline__ void backsolve(double (&x)[N]) const {
+#pragma unroll
+        for (int k = 0; k < N; ++k) {
+            const double xk = x[k];
+#pragma unroll
+            for (int i = k + 1; i < N; ++i) x[i] = Arith<F>::msub(a[i + k * N], xk, x[i]);
+        }
+#pragma unroll
+        for (int k = N - 1; k >= 0; --k) {
+            const double xk = F ? x[k] * a[k + k * N] : x[k] / a[k + k * N];
+            x[k] = xk;
+#pragma unroll
+            for (int i = 0; i < k; ++i) x[i] = Arith<F>::msub(a[i + k * N], xk, x[i]);
+        }
+    }
+
+    // ldiv!! with e = 0 (factors.jl:931-936)
+    __device__ __forceinline__ void ldiv(const double (&r)[N], double (&d)[N]) const {
+        double x[N];
+        if (rhs_unscaled<N>(r)) {
+#pragma unroll
+            for (int i = 0; i < N; ++i) x[i] = r[i];
+            backsolve(x);
+#pragma unroll
+            for (int i = 0; i < N; ++i) d[i] = x[i];
+            return;
+        }
+        const int k = rhs_exponent<N>(r, 0);
+#pragma unroll
+        for (int i = 0; i < N; ++i) x[i] = k == 0 ? r[i] : scale2_in(r[i], -k);  // -k in [-6, 1023]
+        backsolve(x);
+#pragma unroll
+        for (int i = 0; i < N; ++i) d[i] = k == 0 ? x[i] : scale2_in(x[i], k);
     }
 };
 
@@ -504,53 +587,82 @@ template <class Fam, bool F, bool Mixed, bool PlainRef = false, bool Qr = false>
     static constexpr int N = Fam::N, M = Fam::M;
     using JS = typename Fam::JState;
     using A = Arith<F>;
+    // The plain step's gradient ratio feeds only the status of a square system, which keeps the
+    // last factorisation's; where the step parks its start iterate and residual (N >= 6, the
+    // kernel's stash), the ratio is formed once, after the last step, instead of at every step.
+    static constexpr bool kDeferGr = (N >= 6) && !Fam::lsq && !Mixed;
     const Fam& fam;
     const GsbMethod& m;
     const GsbOptions& o;
-    double* stash;  // this thread's 2N doubles of shared memory, or nullptr
+    double* stash;  // this thread's 2N doubles of shared memory (required from N = 6), or nullptr
 
     __device__ Solver(const Fam& f, const GsbMethod& mm, const GsbOptions& oo, double* st)
         : fam(f), m(mm), o(oo), stash(st) {}
 
     // While a factor holds the registers, the iterate and the residual wait in shared memory:
     // a volatile store and a volatile load, so that their register copies are free meanwhile.
+    // With aligned rows (PairsOf) the stash is 16-byte aligned and moves two entries at a time.
+    template <int L> __device__ __forceinline__ void put(unsigned a, const double (&v)[L]) const {
+        if constexpr (PairsOf<Fam>::value && L % 2 == 0) {
+#pragma unroll
+            for (int i = 0; i < L; i += 2) sts2(a + 8u * i, v[i], v[i + 1]);
+        } else {
+#pragma unroll
+            for (int i = 0; i < L; ++i) sts(a + 8u * i, v[i]);
+        }
+    }
+    template <int L> __device__ __forceinline__ void get(unsigned a, double (&v)[L]) const {
+        if constexpr (PairsOf<Fam>::value && L % 2 == 0) {
+#pragma unroll
+            for (int i = 0; i < L; i += 2) lds2(a + 8u * i, v[i], v[i + 1]);
+        } else {
+#pragma unroll
+            for (int i = 0; i < L; ++i) v[i] = lds(a + 8u * i);
+        }
+    }
     __device__ __forceinline__ void park(double (&x)[N], double (&Fx)[M]) const {
         if (stash == nullptr) return;
-        const unsigned a = smem_addr(stash);
-#pragma unroll
-        for (int i = 0; i < N; ++i) sts(a + 8u * i, x[i]);
-#pragma unroll
-        for (int i = 0; i < M; ++i) sts(a + 8u * (N + i), Fx[i]);
+        put<N>(smem_addr(stash), x);
+        put<M>(smem_addr(stash) + 8u * N, Fx);
     }
     __device__ __forceinline__ void park_x(const double (&x)[N]) const {
         if (stash == nullptr) return;
-        const unsigned a = smem_addr(stash);
-#pragma unroll
-        for (int i = 0; i < N; ++i) sts(a + 8u * i, x[i]);
+        put<N>(smem_addr(stash), x);
     }
     __device__ __forceinline__ void park_F(const double (&Fx)[M]) const {
         if (stash == nullptr) return;
-        const unsigned a = smem_addr(stash);
-#pragma unroll
-        for (int i = 0; i < M; ++i) sts(a + 8u * (N + i), Fx[i]);
+        put<M>(smem_addr(stash) + 8u * N, Fx);
     }
     __device__ __forceinline__ void unpark_x(double (&x)[N]) const {
         if (stash == nullptr) return;
-        const unsigned a = smem_addr(stash);
-#pragma unroll
-        for (int i = 0; i < N; ++i) x[i] = lds(a + 8u * i);
+        get<N>(smem_addr(stash), x);
     }
     __device__ __forceinline__ void unpark_F(double (&Fx)[M]) const {
         if (stash == nullptr) return;
-        const unsigned a = smem_addr(stash);
-#pragma unroll
-        for (int i = 0; i < M; ++i) Fx[i] = lds(a + 8u * (N + i));
+        get<M>(smem_addr(stash) + 8u * N, Fx);
     }
 
     __device__ __forceinline__ bool has_merit() const { return m.globalization == GSB_BACKTRACKING; }
 
     // J v as a left fold over the columns (the SMatrix product of the held Jacobian).
     __device__ __forceinline__ void jmul(const JS& js, const double (&v)[N], double (&out)[M]) const {
+        if constexpr (PairsOf<Fam>::value) {
+#pragma unroll
+            for (int i = 0; i < M; i += 2) {
+                double j0, j1;
+                fam.J2(js, i, 0, j0, j1);
+                double s0 = A::mul(j0, v[0]), s1 = A::mul(j1, v[0]);
+#pragma unroll
+                for (int k = 1; k < N; ++k) {
+                    fam.J2(js, i, k, j0, j1);
+                    s0 = A::madd(j0, v[k], s0);
+                    s1 = A::madd(j1, v[k], s1);
+                }
+                out[i] = s0;
+                out[i + 1] = s1;
+            }
+            return;
+        }
 #pragma unroll
         for (int i = 0; i < M; ++i) {
             double s = A::mul(fam.J(js, i, 0), v[0]);
@@ -563,15 +675,10 @@ template <class Fam, bool F, bool Mixed, bool PlainRef = false, bool Qr = false>
     // grad_ratio_and_norm, src/nonlinear/newton.jl:1287-1298.
     __device__ void grad_ratio_and_norm(const JS& js, const double (&Fx)[M], double fnorm,
                                         double& gr, double& jnorm) const {
-        double s = A::mul(fam.J(js, 0, 0), fam.J(js, 0, 0));
-#pragma unroll
-        for (int k = 0; k < N; ++k)
-#pragma unroll
-            for (int i = 0; i < M; ++i) {
-                if (i == 0 && k == 0) continue;
-                double v = fam.J(js, i, k);
-                s = A::madd(v, v, s);
-            }
+        double s = 0.0;
+        for_each_J(fam, js, [&](int i, int k, double v) {
+            s = (i == 0 && k == 0) ? A::mul(v, v) : A::madd(v, v, s);
+        });
         const double tiny = double(M * N) * kFloatmin;
         if (isfin(s) && s >= tiny) {
             jnorm = sqrt(s);
@@ -604,13 +711,9 @@ template <class Fam, bool F, bool Mixed, bool PlainRef = false, bool Qr = false>
             return;
         }
         double g[N];
-#pragma unroll
-        for (int j = 0; j < N; ++j) {
-            double t = A::mul(fam.J(js, 0, j), Fx[0]);
-#pragma unroll
-            for (int i = 1; i < M; ++i) t = A::madd(fam.J(js, i, j), Fx[i], t);
-            g[j] = t;
-        }
+        for_each_J(fam, js, [&](int i, int j, double v) {
+            g[j] = i == 0 ? A::mul(v, Fx[0]) : A::madd(v, Fx[i], g[j]);
+        });
         double gnorm = rnorm<F, N>(g);
         if (isfin(gnorm) || !(isfin(jnorm) && isfin(fnorm))) {
             gr = __ddiv_rn(__ddiv_rn(gnorm, jnorm), fnorm);
@@ -715,8 +818,19 @@ template <class Fam, bool F, bool Mixed, bool PlainRef = false, bool Qr = false>
             code = (isfin(phi0) && isfin(d0)) ? (d0 > 0.0 ? LINESEARCH_FAILED : STALLED) : NONFINITE;
         } else {
             double tau = jmax(__dmul_rn(4.0 * kEps, fabs(phi0)), 4.0 * 4.9406564584124654e-324);
-            double amin = jmax(__ddiv_rn(tau, fabs(d0)), kFloatmin);
-            alpha = jmin(jmax(alpha, amin), kInf);
+            // The step floor amin = max(tau / |d0|, floatmin) is taken when first needed: an
+            // accepted first trial never reads it, and the start max(1, amin) is 1 whenever
+            // tau <= |d0| (then tau / |d0| <= 1 rounds to at most 1).
+            double amin = kNaN;
+            bool have_amin = false;
+            auto floor_ = [&]() {
+                if (!have_amin) {
+                    amin = jmax(__ddiv_rn(tau, fabs(d0)), kFloatmin);
+                    have_amin = true;
+                }
+                return amin;
+            };
+            if (tau > fabs(d0)) alpha = jmin(jmax(alpha, floor_()), kInf);
             double ap = kNaN, pp = kNaN;
             int frozen = 0, trips = 0;
             code = LINESEARCH_FAILED;
@@ -736,7 +850,7 @@ template <class Fam, bool F, bool Mixed, bool PlainRef = false, bool Qr = false>
                 } else if (frozen >= 2) {
                     code = STALLED;
                     done = true;
-                } else if (alpha <= amin) {
+                } else if (alpha <= floor_()) {
                     code = fabs(__dsub_rn(pa, phi0)) <= tau ? STALLED : LINESEARCH_FAILED;
                     done = true;
                 } else {
@@ -831,8 +945,69 @@ template <class Fam, bool F, bool Mixed, bool PlainRef = false, bool Qr = false>
         return true;
     }
 
+    // d = -(fac \ F) refined (Refinement with the Float64 factor): the direction, then its passes.
+    template <class Fac>
+    __device__ __forceinline__ void refine_neg(double (&d)[N], const Fac& fac, const JS& js,
+                                               const double (&Fx)[M]) const {
+#pragma unroll
+        for (int i = 0; i < N; ++i) d[i] = -d[i];
+        refine(d, fac, js, Fx);
+    }
+
     // The plain step (TF = T), src/nonlinear/newton.jl:1679-1688.
     __device__ void step_plain(DevState& st, double (&x)[N], double (&Fx)[M], StepInfo& info) const {
+        if constexpr (kDeferGr) {
+            // the gradient ratio is formed after the last step (stashed_grad_ratio)
+            JS js;
+            fam.jacobian(x, js);
+            double merit = st.merit;
+            double d[N];
+            bool singular = false;
+            park(x, Fx);
+            if constexpr (Qr) {
+                QRFactor<F, N> fac;
+                fac.factor(fam, js);
+                singular = fac.info > 0;
+                if (!singular) {
+                    unpark_F(Fx);
+                    fac.ldiv(Fx, d);
+                    if constexpr (PlainRef) refine_neg(d, fac, js, Fx);
+                }
+            } else {
+                // the register factor without exchanges or scaling, else (rarely) the factor
+                // with both in thread-local memory: the same bits
+                DiagLU<F, N> fac;
+                if (fac.factor(fam, js)) {
+                    unpark_F(Fx);
+                    fac.ldiv(Fx, d);
+                    if constexpr (PlainRef) refine_neg(d, fac, js, Fx);
+                } else {
+                    LocalLU<F, N> lf;
+                    lf.factor(fam, js);
+                    singular = lf.info > 0;
+                    if (!singular) {
+                        unpark_F(Fx);
+                        lf.ldiv(Fx, d);
+                        if constexpr (PlainRef) refine_neg(d, lf, js, Fx);
+                    }
+                }
+            }
+            if (singular) {
+                unpark_x(x);
+                unpark_F(Fx);
+                info = {SINGULAR, rnorm<F, M>(Fx), 0.0, 0, false, false, false};
+            } else {
+                if constexpr (!PlainRef) {
+#pragma unroll
+                    for (int i = 0; i < N; ++i) d[i] = -d[i];
+                }
+                unpark_x(x);
+                globalize(x, Fx, d, !PlainRef, merit, info);
+            }
+            st.merit = merit;
+            st.fnorm = info.fnorm;
+            return;
+        }
         double fnorm = residual_norm(st, Fx);
         JS js;
         fam.jacobian(x, js);
@@ -982,9 +1157,45 @@ template <class Fam, bool F, bool Mixed, bool PlainRef = false, bool Qr = false>
         return ftest <= jmax(o.f_abstol, __dmul_rn(o.f_reltol, ftest0));
     }
 
+    // The gradient ratio of the last step (grad_ratio_and_norm, newton.jl:1287-1298) from the
+    // iterate and residual that step parked at its start: the Jacobian there, the two sums that
+    // the factor's load would have folded (the squares of J's entries in column order, J' F), in
+    // the same order, and the residual norm that the step read (its merit is norm2 of that
+    // residual, the same fold), so the ratio has the bits the step itself would have formed.
+    __device__ double stashed_grad_ratio() const {
+        double xs[N], Fs[M];
+        unpark_x(xs);
+        unpark_F(Fs);
+        double fnorm;
+        if (has_merit()) {
+            const double m2 = norm2<F, M>(Fs);
+            fnorm = (isfin(m2) && m2 >= double(M) * kFloatmin) ? sqrt(m2) : rnorm<F, M>(Fs);
+        } else {
+            fnorm = rnorm<F, M>(Fs);
+        }
+        JS js;
+        fam.jacobian(xs, js);
+        double s = 0.0, g[N];
+        for_each_J(fam, js, [&](int i, int k, double v) {
+            s = (i == 0 && k == 0) ? A::mul(v, v) : A::madd(v, v, s);
+            g[k] = i == 0 ? A::mul(v, Fs[0]) : A::madd(v, Fs[i], g[k]);
+        });
+        double gr, jn;
+        if (!grad_ratio_fast(s, g, fnorm, gr, jn)) grad_ratio_and_norm(js, Fs, fnorm, gr, jn);
+        return gr;
+    }
+
     // solve!!, src/nonlinear/solver.jl:277-378. Returns the status; `gr` is the gradratio of
     // the last factorisation (newton_finish!!, src/nonlinear/newton.jl:1165-1184).
     __device__ DevStatus solve(double (&x)[N], double& gr_out) const {
+        DevStatus s = solve_steps(x, gr_out);
+        if constexpr (kDeferGr) {
+            if (s.iterations > 0) gr_out = stashed_grad_ratio();
+        }
+        return s;
+    }
+
+    __device__ DevStatus solve_steps(double (&x)[N], double& gr_out) const {
         double Fx[M];
         fam.F(x, Fx);
         double n2 = norm2<F, M>(Fx);

@@ -160,6 +160,13 @@ __device__ __forceinline__ double lds(unsigned addr) {
 __device__ __forceinline__ void sts(unsigned addr, double v) {
     asm volatile("st.shared.f64 [%0], %1;" ::"r"(addr), "d"(v) : "memory");
 }
+// Two consecutive doubles at a 16-byte aligned shared address, as one 16-byte access.
+__device__ __forceinline__ void lds2(unsigned addr, double& v0, double& v1) {
+    asm volatile("ld.shared.v2.f64 {%0, %1}, [%2];" : "=d"(v0), "=d"(v1) : "r"(addr));
+}
+__device__ __forceinline__ void sts2(unsigned addr, double v0, double v1) {
+    asm volatile("st.shared.v2.f64 [%0], {%1, %2};" ::"r"(addr), "d"(v0), "d"(v1) : "memory");
+}
 
 // Julia's `exponent` of a finite nonzero value.
 __device__ __forceinline__ int jexponent(double x) { return ilogb(x); }
@@ -226,6 +233,16 @@ template <int L> __device__ __forceinline__ int matrix_exponent(const double (&a
     return lo != 0 ? -1023 : 0;           // subnormal, or all zero
 }
 
+// A key whose unsigned order is that of |x| between values of distinct high words (the high
+// 32 bits with the sign shifted out): key(x) < key(y) implies |x| < |y|; a NaN has a key above
+// every finite value's.
+__device__ __forceinline__ unsigned mag_key(double x) { return (unsigned)__double2hiint(x) << 1; }
+__device__ __forceinline__ unsigned mag_key(float x) { return __float_as_uint(x) << 1; }
+
+// The correctly rounded reciprocal: the bits of 1 / x.
+__device__ __forceinline__ double crcp(double x) { return __drcp_rn(x); }
+__device__ __forceinline__ float crcp(float x) { return __frcp_rn(x); }
+
 // headroom(n) = 2 + ceil(log2 n) (src/linear/factors.jl:890), a constant of the size.
 __host__ __device__ constexpr int headroom(int n) {
     int b = 0;
@@ -244,6 +261,21 @@ template <int L> __device__ __forceinline__ int rhs_exponent(const double (&r)[L
     int a = m > 0 ? 0 : (m < lo ? lo : m);
     int b = m - (1023 - headroom(L));
     return a > b ? a : b;
+}
+
+// True when rhs_exponent(r, 0) is 0: with e = 0 that exponent is max(0, m - (1023 - headroom)),
+// m the exponent of the largest |r_i| (0 when that is Inf or NaN), so it is 0 unless the largest
+// |r_i| is finite with an exponent above 1023 - headroom. Decided on the exponent field of the
+// largest high word, as matrix_exponent reads it.
+template <int L> __device__ __forceinline__ bool rhs_unscaled(const double (&r)[L]) {
+    unsigned h = 0;
+#pragma unroll
+    for (int i = 0; i < L; ++i) {
+        const unsigned v = (unsigned)__double2hiint(r[i]) << 1;
+        h = h > v ? h : v;
+    }
+    const int field = (int)(h >> 21);
+    return field == 2047 || field - 1023 <= 1023 - headroom(L);
 }
 
 static __device__ __noinline__ double ldexp2_slow(double x, int e) { return ldexp2(x, e); }

@@ -190,12 +190,16 @@ typedef struct {
     int64_t counts[6];
 } GsbTally;
 
-/* BatchSummary{Float64}, src/nonlinear/batched.jl:63-69. */
+/* BatchSummary{Float64} (src/nonlinear/batched.jl:63-69) with Julia's field layout: offsets
+ * fnorm 0, all_converged 8 (Bool), failure_count 16, max_iterations 24 (Int32),
+ * total_iterations 32; size 40, alignment 8. A Ref{BatchSummary{Float64}} is passed by pointer. */
 typedef struct {
     double fnorm;
-    int32_t all_converged;
-    int32_t max_iterations;
+    uint8_t all_converged;
+    uint8_t pad0_[7];
     int64_t failure_count;
+    int32_t max_iterations;
+    int32_t pad1_;
     int64_t total_iterations;
 } GsbSummary;
 
@@ -249,20 +253,24 @@ GSB_API int gsb_solve_batch(const GsbProblem* prob, const GsbMethod* method, con
  * Synchronises `stream`. */
 GSB_API int gsb_batch_summary(const GsbStatus64* S, int64_t nsys, void* stream, GsbSummary* out);
 
-/* Wait for the work queued on `stream`. */
+/* Wait for the work queued on `stream`. Returns GSB_ERR_CUDA if a batch kernel reported that a
+ * bounded wait for its parameter staging copies ran out (its systems were then left unsolved; no
+ * such wait is expected to run out). */
 GSB_API int gsb_synchronize(void* stream);
 
 /*
  * The count form of gsb_solve_batch for callers that cannot allocate device memory: a host whose
  * memory manager has reserved the whole device heap for its own pool, or a loop that cannot take
- * the device-wide synchronisation of cudaMalloc. No counterpart in the reference: it is the count
- * form (src/nonlinear/batched.jl:289-307) with its working memory moved out of the allocator.
+ * the device-wide synchronisation of cudaMalloc. It has no counterpart in the reference: it is
+ * the count form with its working memory in a static device array of this library instead of
+ * the allocator.
  *
  * It solves in place like gsb_solve_batch with s_kind GSB_CODES: X receives the iterates, `codes`
  * (uint8_t[nsys], device) the ReturnCodes, and *tally (host, required) the six counts. The six
- * counters and the permutation check of `order` live in one static device array of this library
- * (2 MiB, held by every device that loads the library until the process exits), so the call
- * allocates nothing: no cudaMalloc, no host heap. Limit: with `order`, nsys may be at most
+ * counters, the permutation check of `order` and the kernel's staging-fault word live in one
+ * static device array of this library (2 MiB, held by every device that loads the library until
+ * the process exits), so a successful call allocates nothing: no cudaMalloc, no host heap (an
+ * error's message text may allocate). Limit: with `order`, nsys may be at most
  * GSB_NOALLOC_MAX_ORDERED (16,777,216); beyond it the call returns GSB_ERR_DIMENSION before any
  * launch. Without `order` there is no limit. The first call on a device also looks up the
  * array's device address; make that first call before any stream capture on that device. Every

@@ -36,6 +36,16 @@ def test_status_layout(gsb):
     assert gsb.SOLVER_STATUS_DTYPE.itemsize == 72
 
 
+def test_summary_layout(gsb):
+    # BatchSummary{Float64}, src/nonlinear/batched.jl:63-69: fnorm::Float64, all_converged::Bool,
+    # failure_count::Int, max_iterations::Int32, total_iterations::Int (Julia's C layout)
+    S = gsb.abi.GsbSummary
+    offsets = {f: getattr(S, f).offset for f, _ in S._fields_}
+    assert ctypes.sizeof(S) == 40
+    assert [offsets[f] for f in ("fnorm", "all_converged", "failure_count", "max_iterations",
+                                 "total_iterations")] == [0, 8, 16, 24, 32]
+
+
 def test_defaults_match_reference(gsb):
     lib = gsb.load_library()
     o = gsb.abi.GsbOptions()

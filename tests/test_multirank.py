@@ -83,3 +83,32 @@ def test_one_rank_is_the_identity():
     r = bench.Ranks(1)
     assert r.max(3.5) == 3.5 and r.sum(7.0) == 7.0
     r.barrier()
+
+
+def _bench_line(*args):
+    import json
+    import subprocess
+
+    env = dict(os.environ)
+    for k in ("RANK", "WORLD_SIZE", "LOCAL_RANK", "MASTER_ADDR", "MASTER_PORT"):
+        env.pop(k, None)
+    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), *args], env=env,
+                         capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = [ln for ln in out.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1, out.stdout
+    return json.loads(lines[0])
+
+
+def test_bench_starts_its_own_ranks():
+    """`bench.py --gpus 2` with no launcher around it starts two ranks under torch.distributed.run;
+    their collectives (barrier, maximum, sum) run over gloo, and rank 0 alone prints the world
+    size it saw."""
+    line = _bench_line("--gpus", "2", "--launch-check")
+    assert line["n_gpus"] == 2 and line["max_rank"] == 1.0 and line["ranks_counted"] == 2.0
+
+
+def test_reference_arm_reports_the_world_size():
+    line = _bench_line("--gpus", "2", "--impl", "reference", "--steps", "1", "--warmup", "0",
+                       "--nsys", "2048")
+    assert line["impl"] == "reference" and line["n_gpus"] == 2

@@ -879,8 +879,8 @@ def run_workload(args):
                                                   1 + _trials(so))))
             bytes_total = bytes_per_system(3) * nsys
         else:
-            fr = np.abs(st["fnorm"][:ns] - so["fnorm"]) / np.maximum(so["fnorm"], 1e-300)
-            ok = (st["code"][:ns] == so["code"]) & (fr <= np.where(so["code"] == 0, 1e-10, 1e-9))
+            # solved: the oracle's code and the iterate within 1e-10 of the oracle's
+            ok = (st["code"][:ns] == so["code"]) & (rel_err(x[:ns], xo) <= REL_TOL)
             flops = float(np.mean(lm_flops_per_system(
                 64, 6, st["iterations"].astype(np.int64), st["step_failures"].astype(np.int64))))
             flops *= nsys
@@ -889,24 +889,36 @@ def run_workload(args):
         with Clocks(0) as clk:
             ms = _events_ms(step, args.steps, args.warmup, stream)
             if args.workload == "c2":
-                # the mixed form: FP32 stacked factor with FP64 refinement
-                m32 = G.Newton(linsolve=G.QRFactorization("float32"),
-                               globalization=G.LevenbergMarquardt())
+                # the other forms of the fit: FP64 with unfused arithmetic (the oracle's rounding,
+                # bit for bit) and the FP32 stacked factor with FP64 refinement
+                others = {
+                    "fp64_unfused": G.Newton(linsolve=G.QRFactorization(),
+                                             globalization=G.LevenbergMarquardt(),
+                                             arithmetic="unfused"),
+                    "fp32_qr_refinement": G.Newton(linsolve=G.QRFactorization("float32"),
+                                                   globalization=G.LevenbergMarquardt()),
+                }
+                for fname, mo in others.items():
+                    def step_o(mo=mo):
+                        X.copy_(X0)
+                        G.solve_batch(X, S, prob, mo, ps, options=opts)
 
-                def step32():
-                    X.copy_(X0)
-                    G.solve_batch(X, S, prob, m32, ps, options=opts)
-
-                ms32 = _events_ms(step32, args.steps, args.warmup, stream)
-                step32()
-                st32 = G.statuses(S)
-                fr32 = np.abs(st32["fnorm"][:ns] - so["fnorm"]) / np.maximum(so["fnorm"], 1e-300)
-                ok32 = (st32["code"][:ns] == so["code"]) & (
-                    fr32 <= np.where(so["code"] == 0, 1e-10, 1e-9))
-                forms["fp32_qr_refinement"] = {
-                    "systems_per_s": float(np.mean(ok32)) * nsys / (ms32 * 1e-3), "ms_per_step": ms32,
-                    "solved_fraction": float(np.mean(ok32)), "oracle_checked_systems": ns}
+                    ms_o = _events_ms(step_o, args.steps, args.warmup, stream)
+                    step_o()
+                    st_o = G.statuses(S)
+                    x_o = X.cpu().numpy()
+                    ok_o = (st_o["code"][:ns] == so["code"]) & (rel_err(x_o[:ns], xo) <= REL_TOL)
+                    forms[fname] = {
+                        "systems_per_s": float(np.mean(ok_o)) * nsys / (ms_o * 1e-3),
+                        "ms_per_step": ms_o, "solved_fraction": float(np.mean(ok_o)),
+                        "oracle_checked_systems": ns, "method": mo}
         clocks = clk.summary()
+        # the end-to-end leg runs the form with the most systems solved per second
+        chosen_m = method
+        best = solved_frac * nsys / (ms * 1e-3)
+        for f in forms.values():
+            if f["systems_per_s"] > best:
+                best, chosen_m = f["systems_per_s"], f["method"]
         value = solved_frac * nsys / (ms * 1e-3)
         # the solve alone: the step minus the copy of the start iterates
         kms = ms - _events_ms(lambda: X.copy_(X0), 20, 2, stream)
@@ -920,7 +932,7 @@ def run_workload(args):
         def e2e():
             Xe.copy_(x_pin, non_blocking=True)
             Pe.copy_(p_pin, non_blocking=True)
-            G.solve_batch(Xe, S, prob, method, G.PerSystem(Pe), options=opts)
+            G.solve_batch(Xe, S, prob, chosen_m, G.PerSystem(Pe), options=opts)
             x_out.copy_(Xe, non_blocking=True)
             s_out.copy_(S, non_blocking=True)
 
@@ -934,11 +946,16 @@ def run_workload(args):
                          "oracle_checked_systems": ns}
         launches = args.steps
         chosen = "fp64"
-        if "fp32_qr_refinement" in forms and forms["fp32_qr_refinement"]["systems_per_s"] > value:
-            chosen = "fp32_qr_refinement"
+        for fname in ("fp64_unfused", "fp32_qr_refinement"):
+            if fname in forms and forms[fname]["systems_per_s"] > forms[chosen]["systems_per_s"]:
+                chosen = fname
+        if chosen != "fp64":
             value = forms[chosen]["systems_per_s"]
             ms = forms[chosen]["ms_per_step"]
+        for f in forms.values():
+            f.pop("method", None)
         if args.workload == "c2":
+            forms["chosen"] = chosen
             forms["chosen_over_plain"] = value / forms["fp64"]["systems_per_s"]
     else:
         from workloads import c4

@@ -17,6 +17,7 @@
 #pragma once
 
 #include "../../include/gsb.h"
+#include "gsb_exp.h"
 #include "gsb_newton.cuh"
 #include "gsb_numerics.cuh"
 
@@ -34,13 +35,14 @@ template <int M_> struct ExpSum3 {
     __device__ __forceinline__ double yv(int i) const { return lds(smem_addr(y) + 8u * i); }
     __device__ __forceinline__ double tv(int i) const { return lds(smem_addr(t) + 8u * i); }
 
-    // F_i(x): ((a1 e1 + a2 e2) + a3 e3) - y_i with e_j = exp(-(b_j t_i)).
+    // F_i(x): ((a1 e1 + a2 e2) + a3 e3) - y_i with e_j = exp(-(b_j t_i)), exp being
+    // gsb_exp::exp (Tang's method, the same bits on the host).
     template <bool F> __device__ __forceinline__ double residual(const double (&x)[6], int i) const {
         using A = Arith<F>;
         const double ti = tv(i);
-        const double e1 = exp(-A::mul(x[1], ti));
-        const double e2 = exp(-A::mul(x[3], ti));
-        const double e3 = exp(-A::mul(x[5], ti));
+        const double e1 = gsb_exp::exp(-A::mul(x[1], ti));
+        const double e2 = gsb_exp::exp(-A::mul(x[3], ti));
+        const double e3 = gsb_exp::exp(-A::mul(x[5], ti));
         return A::sub(A::madd(x[4], e3, A::madd(x[2], e2, A::mul(x[0], e1))), yv(i));
     }
 
@@ -51,9 +53,9 @@ template <int M_> struct ExpSum3 {
     __device__ __forceinline__ double row(const double (&x)[6], int i, double (&J)[6]) const {
         using A = Arith<F>;
         const double ti = tv(i);
-        const double e1 = exp(-A::mul(x[1], ti));
-        const double e2 = exp(-A::mul(x[3], ti));
-        const double e3 = exp(-A::mul(x[5], ti));
+        const double e1 = gsb_exp::exp(-A::mul(x[1], ti));
+        const double e2 = gsb_exp::exp(-A::mul(x[3], ti));
+        const double e3 = gsb_exp::exp(-A::mul(x[5], ti));
         J[0] = e1;
         J[1] = A::mul(A::mul(e1, -ti), x[0]);
         J[2] = e2;

@@ -4,6 +4,8 @@
 // runs both on the same inputs. The batch loop splits the systems into one contiguous range per
 // thread, the static schedule of the reference's own host R1 loop
 // (`Threads.@threads :static`, scripts/r2_throughput.jl:107-136).
+#include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <thread>
 #include <vector>
@@ -156,6 +158,61 @@ extern "C" {
 int oracle_abi_version(void) { return GSB_ABI_VERSION; }
 
 int oracle_max_threads(void) { return (int)std::thread::hardware_concurrency(); }
+
+// The error of gsb_exp::exp (the exponential-sum family's exp, shared with the batch kernel)
+// against long double expl on n arguments: a quarter uniform in [-1, 1], a quarter in [-40, 5]
+// (the fit's range) and half uniform in [lo, hi]. Writes the largest error in ulp of the exact
+// value (as far as expl resolves it), its argument and the count of results that differ from
+// expl rounded to double. Normal results only.
+int oracle_exp_check(int64_t n, uint64_t seed, double lo, double hi, double* max_ulp,
+                     double* worst_x, int64_t* not_nearest) {
+    const int nt = std::max(1, (int)std::thread::hardware_concurrency());
+    std::vector<double> mu(nt, 0.0), wx(nt, 0.0);
+    std::vector<int64_t> nn(nt, 0);
+    std::vector<std::thread> th;
+    for (int w = 0; w < nt; ++w) {
+        th.emplace_back([&, w] {
+            uint64_t st = seed * 0x9E3779B97F4A7C15ull + (uint64_t)w * 0xD1B54A32D192ED03ull + 1;
+            auto next = [&] {  // splitmix64
+                uint64_t z = (st += 0x9E3779B97F4A7C15ull);
+                z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+                z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+                return (double)((z ^ (z >> 31)) >> 11) * 0x1.0p-53;
+            };
+            for (int64_t i = w; i < n; i += nt) {
+                const double u = next();
+                const double x = (i % 4 == 0) ? -1.0 + 2.0 * u
+                                 : (i % 4 == 1) ? -40.0 + 45.0 * u : lo + (hi - lo) * u;
+                const double a = gsb_exp::exp(x);
+                const long double r = expl((long double)x);
+                if (!(r >= (long double)2.2250738585072014e-308) || !std::isfinite((double)r))
+                    continue;
+                int ex;
+                frexpl(r, &ex);
+                const double err = (double)(fabsl((long double)a - r) / ldexpl(1.0L, ex - 53));
+                if (err > mu[w]) {
+                    mu[w] = err;
+                    wx[w] = x;
+                }
+                if ((double)r != a) ++nn[w];
+            }
+        });
+    }
+    for (auto& t : th) t.join();
+    *max_ulp = 0.0;
+    *worst_x = 0.0;
+    *not_nearest = 0;
+    for (int w = 0; w < nt; ++w) {
+        if (mu[w] > *max_ulp) {
+            *max_ulp = mu[w];
+            *worst_x = wx[w];
+        }
+        *not_nearest += nn[w];
+    }
+    return 0;
+}
+
+double oracle_exp(double x) { return gsb_exp::exp(x); }
 
 // The CPU batch over host arrays, with the arguments of gsb_solve_batch; nthreads <= 0 takes
 // every hardware thread.

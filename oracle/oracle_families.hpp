@@ -6,6 +6,7 @@
 
 #include <cmath>
 
+#include "../geometricsolvers.jl_b200/csrc/gsb_exp.h"
 #include "oracle_dual.hpp"
 
 namespace orc {
@@ -27,6 +28,16 @@ template <int K> inline Dual<K> fmac(double c, const Dual<K>& x, const Dual<K>& 
 
 inline double exp(double x) { return std::exp(x); }
 inline double sqrt(double x) { return std::sqrt(x); }
+
+// The exponential of the exponential-sum family: the batch kernel's own (gsb_exp.h, Tang's
+// table-driven method, the same bits on the host as on the device), so that the fit is checked
+// bit for bit. The reference evaluates Julia's Base.exp, which neither the C library's exp nor
+// this one reproduces in every last bit; every other exp of the oracle is the C library's.
+inline double fam_exp(double x) { return gsb_exp::exp(x); }
+template <int K> inline Dual<K> fam_exp(const Dual<K>& a) {
+    const double e = gsb_exp::exp(a.v);
+    return chain(a, e, e);
+}
 
 // ─── GSB_FAMILY_CUBIC_AFFINE: F(x) = A x + 0.1 x.^3 - b, p = (A column-major, b) ───────────
 // Each row is the fused dot product fma(A_in, x_n, ... fma(A_i2, x_2, A_i1 x_1)), then
@@ -57,9 +68,9 @@ template <int M_> struct ExpSum3 {
     const double* t;
     template <class S> void F(const S* x, S* out) const {
         for (int i = 0; i < M; ++i) {
-            S e1 = exp(-(x[1] * t[i]));
-            S e2 = exp(-(x[3] * t[i]));
-            S e3 = exp(-(x[5] * t[i]));
+            S e1 = fam_exp(-(x[1] * t[i]));
+            S e2 = fam_exp(-(x[3] * t[i]));
+            S e3 = fam_exp(-(x[5] * t[i]));
             out[i] = ((x[0] * e1 + x[2] * e2) + x[4] * e3) - y[i];
         }
     }

@@ -145,24 +145,29 @@ __device__ __forceinline__ void stage_arrive(uint64_t* bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
 }
 
-__device__ __forceinline__ void store_status(void* S, int64_t idx, const DevStatus& s, double gr) {
-    unsigned long long* w = reinterpret_cast<unsigned long long*>(
-        reinterpret_cast<unsigned char*>(S) + idx * 72);
-    unsigned long long w0 = (unsigned long long)(unsigned char)s.code |
-                            ((unsigned long long)(unsigned int)s.iterations << 32);
-    unsigned long long w3 = (unsigned long long)(unsigned int)s.step_failures |
-                            ((unsigned long long)(s.promoted ? 1u : 0u) << 32) |
-                            ((unsigned long long)(s.stationary ? 1u : 0u) << 40);
-    unsigned long long w4 = (unsigned long long)(unsigned int)(-1);
-    w[0] = w0;
+// The 72-byte status record (GsbStatus64) of a system as nine 8-byte words.
+__device__ __forceinline__ void status_words(const DevStatus& s, double gr, unsigned long long (&w)[9]) {
+    w[0] = (unsigned long long)(unsigned char)s.code |
+           ((unsigned long long)(unsigned int)s.iterations << 32);
     w[1] = (unsigned long long)__double_as_longlong(s.fnorm);
     w[2] = (unsigned long long)__double_as_longlong(s.stepnorm);
-    w[3] = w3;
-    w[4] = w4;
+    w[3] = (unsigned long long)(unsigned int)s.step_failures |
+           ((unsigned long long)(s.promoted ? 1u : 0u) << 32) |
+           ((unsigned long long)(s.stationary ? 1u : 0u) << 40);
+    w[4] = (unsigned long long)(unsigned int)(-1);
     w[5] = (unsigned long long)__double_as_longlong(kNaN);
     w[6] = (unsigned long long)__double_as_longlong(gr);
     w[7] = (unsigned long long)__double_as_longlong(s.rate);
     w[8] = (unsigned long long)(s.contracted ? 1u : 0u);
+}
+
+__device__ __forceinline__ void store_status(void* S, int64_t idx, const DevStatus& s, double gr) {
+    unsigned long long* o = reinterpret_cast<unsigned long long*>(
+        reinterpret_cast<unsigned char*>(S) + idx * 72);
+    unsigned long long w[9];
+    status_words(s, gr, w);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) o[k] = w[k];
 }
 
 __device__ __forceinline__ void tally_code(unsigned long long* tally, int code) {
@@ -210,92 +215,178 @@ template <class Fam, bool Mixed> constexpr int min_blocks() {
 #endif
 }
 
+// The Newton solve of one system by its thread, once its parameter row is staged.
+template <class Fam, bool F, bool Mixed, bool PlainRef, bool Qr>
+__device__ __forceinline__ DevStatus solve_one(const GsbMethod& m, const GsbOptions& o,
+                                               const double* smem, double* prow,
+                                               double (&x)[Fam::N], double& gr) {
+    constexpr int N = Fam::N, NP = Fam::NP;
+    Fam fam{prow};
+    if constexpr (SharedLen<Fam>::value > 0) fam.a = smem;
+    Solver<Fam, F, Mixed, PlainRef, Qr> sv(fam, m, o, N >= 6 ? prow + NP : nullptr);
+    return sv.solve(x, gr);
+}
+
+// A warp's stores of 32 consecutive systems (base .. base + 31, AoS iterates, 72-byte statuses,
+// both arrays 16-byte aligned): each lane puts its status words and then its iterate into `buf`
+// (shared memory the warp no longer reads, 16-byte aligned, at least 32 * max(9, N) doubles),
+// and the warp copies the 2,304 status bytes and the 32 * 8N iterate bytes out as 16-byte stores
+// that fill whole lines.
+template <int N>
+__device__ __forceinline__ void store_warp(const Launch& L, int64_t base, int lane, double* buf,
+                                           const double (&x)[N], const DevStatus& s, double gr) {
+    static_assert((N * 8) % 16 == 0, "16-byte pieces of the iterates");
+    const unsigned b = smem_addr(buf);
+    unsigned long long w[9];
+    status_words(s, gr, w);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) sts(b + 8u * (lane * 9 + k), __longlong_as_double((long long)w[k]));
+    __syncwarp();
+    unsigned char* sb = reinterpret_cast<unsigned char*>(L.S) + base * 72;
+#pragma unroll
+    for (int q = lane; q < 144; q += 32) {
+        double v0, v1;
+        lds2(b + 16u * q, v0, v1);
+        asm volatile("st.global.v2.f64 [%0], {%1, %2};" ::"l"(sb + 16 * q), "d"(v0), "d"(v1) : "memory");
+    }
+    __syncwarp();
+#pragma unroll
+    for (int k = 0; k < N; ++k) sts(b + 8u * (lane * N + k), x[k]);
+    __syncwarp();
+    double* xb = L.X + base * N;
+#pragma unroll
+    for (int q = lane; q < 32 * N / 2; q += 32) {
+        double v0, v1;
+        lds2(b + 16u * q, v0, v1);
+        asm volatile("st.global.v2.f64 [%0], {%1, %2};" ::"l"(xb + 2 * q), "d"(v0), "d"(v1) : "memory");
+    }
+}
+
+// The thread's stores of its system's iterate and status (or code).
+template <int N>
+__device__ __forceinline__ void store_one(const Launch& L, int64_t idx, const double (&x)[N],
+                                          const DevStatus& s, double gr) {
+    double* xb = x_block(L, idx, N);
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+        if (L.x_layout == GSB_SOA) L.X[(int64_t)k * L.nsys + idx] = x[k];
+        else xb[k] = x[k];
+    }
+    if (L.s_kind == GSB_STATUS64) store_status(L.S, idx, s, gr);
+    else reinterpret_cast<unsigned char*>(L.S)[idx] = (unsigned char)s.code;
+}
+
 template <class Fam, bool F, bool Mixed, bool PlainRef, bool Persistent, bool Qr = false>
 __global__ void __launch_bounds__(kThreads, (min_blocks<Fam, Mixed>())) newton_kernel(const __grid_constant__ GsbMethod m,
                                  const __grid_constant__ GsbOptions o,
                                  const __grid_constant__ Launch L) {
     extern __shared__ __align__(16) double smem[];
     constexpr int N = Fam::N, NP = Fam::NP, RS = newton_row_stride<Fam>();
-    constexpr bool kBulk = PairsOf<Fam>::value;
     // a family's block shared by the batch (BatchParams) first, then one row per thread
     constexpr int SH = SharedLen<Fam>::value, SHP = ((SH + 1) / 2) * 2;
     const int tid = threadIdx.x;
     double* rows = smem + SHP;
     double* prow = rows + tid * RS;
-    __shared__ __align__(8) uint64_t bar;  // completion of a chunk's row copies (kBulk)
-    uint32_t phase = 0;
     if constexpr (SH > 0) {
         for (int q = tid; q < SH; q += kThreads) smem[q] = __ldg(L.shared + q);
-    }
-    if constexpr (kBulk) {
-        if (tid == 0) {
-            umma::mbar_init(&bar, kThreads);
-            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        }
         __syncthreads();
     }
-    for_each_chunk<Persistent>(L, kThreads, [&](int64_t base, const Range& r) {
-        const int64_t i = base + tid;
-        double x[N];
-        if constexpr (kBulk) {
-            // every thread stages its own system's row and arrives; the CTA waits for all,
-            // with the thread's iterate loads in flight meanwhile
-            if (i < r.n) {
+    if constexpr (PairsOf<Fam>::value) {
+        // Each warp works on its own: it stages the rows of its 32 systems (one bulk copy per
+        // system, completing on the warp's mbarrier), solves them, and takes its next 32 (from a
+        // fixed stride over the grid's warps, or from the launch's work queue), so that one
+        // warp's wait for its copies overlaps the arithmetic of the others and no warp waits for
+        // the slowest system of another. The grid holds the resident CTAs only.
+        constexpr int W = kThreads / 32;
+        const int warp = tid >> 5, lane = tid & 31;
+        __shared__ __align__(8) uint64_t wbar[W];
+        if (lane == 0) {
+            umma::mbar_init(&wbar[warp], 32);
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        }
+        __syncwarp();
+        const Range r = launch_range(L);
+        uint32_t phase = 0;
+        int64_t c = (int64_t)blockIdx.x * W + warp;
+        while (true) {
+            if constexpr (Persistent) {
+                unsigned long long t = 0;
+                if (lane == 0) t = atomicAdd(L.queue, 1ull);
+                c = (int64_t)__shfl_sync(0xffffffffu, t, 0);
+            }
+            if (c * 32 >= r.n) break;
+            const int64_t i = c * 32 + lane;
+            const bool mine = i < r.n;
+            const int64_t idx = mine ? (r.order ? r.order[i] - L.order_base : i) : 0;
+            double x[N];
+            if (mine) {
+                if (L.p_layout == GSB_SOA) {
+#pragma unroll 4
+                    for (int k = 0; k < NP; ++k) prow[k] = __ldg(L.P + (int64_t)k * L.nsys + idx);
+                    stage_arrive(&wbar[warp]);
+                } else {
+                    stage_row_bulk<NP>(prow, param_block(L, idx, NP), &wbar[warp]);
+                }
+                load_x<N>(L, idx, x);  // in flight while the copies land
+            } else {
+                stage_arrive(&wbar[warp]);
+            }
+            const bool staged =
+                __all_sync(0xffffffffu, umma::mbar_wait(&wbar[warp], phase, kStageWaitPolls));
+            phase ^= 1u;
+            if (!staged) {
+                // the copies did not land: record it, give them a second bounded wait, and
+                // leave this warp's systems unsolved
+                if (L.fault && lane == 0) *reinterpret_cast<volatile unsigned*>(L.fault) = 1u;
+                umma::mbar_wait(&wbar[warp], phase ^ 1u, kStageWaitPolls);
+                break;
+            }
+            __syncwarp();  // the lanes' own stores of their rows (SoA) before any read
+            DevStatus st{};
+            double gr = kNaN;
+            if (mine) st = solve_one<Fam, F, Mixed, PlainRef, Qr>(m, o, smem, prow, x, gr);
+            __syncwarp();  // the rows are free again
+            static_assert(RS >= 9 && RS >= N, "a warp's rows hold its 32 statuses and iterates");
+            if (c * 32 + 32 <= r.n && r.order == nullptr && L.s_kind == GSB_STATUS64 &&
+                L.x_layout == GSB_AOS && L.x_off == nullptr &&
+                ((reinterpret_cast<uintptr_t>(L.S) | reinterpret_cast<uintptr_t>(L.X)) & 15u) == 0) {
+                // whole lines: the warp's statuses and iterates pass through its own free rows
+                store_warp<N>(L, c * 32, lane, rows + warp * 32 * RS, x, st, gr);
+                __syncwarp();
+            } else if (mine) {
+                store_one<N>(L, idx, x, st, gr);
+            }
+            if (L.tally && mine) tally_code(L.tally, st.code);
+            if constexpr (!Persistent) c += (int64_t)gridDim.x * W;
+        }
+        return;
+    } else {
+        for_each_chunk<Persistent>(L, kThreads, [&](int64_t base, const Range& r) {
+            const int64_t i = base + tid;
+            if (r.order == nullptr && L.p_layout == GSB_AOS && L.p_off == nullptr) {
+                stage_aos<NP, RS, kThreads>(rows, L.P + base * NP, r.n - base, tid);
+            } else if (i < r.n) {
                 const int64_t idx = r.order ? r.order[i] - L.order_base : i;
                 if (L.p_layout == GSB_SOA) {
 #pragma unroll 4
                     for (int k = 0; k < NP; ++k) prow[k] = __ldg(L.P + (int64_t)k * L.nsys + idx);
-                    stage_arrive(&bar);
                 } else {
-                    stage_row_bulk<NP>(prow, param_block(L, idx, NP), &bar);
+                    const double* pb = param_block(L, idx, NP);
+#pragma unroll 4
+                    for (int k = 0; k < NP; ++k) prow[k] = __ldg(pb + k);
                 }
-            } else {
-                stage_arrive(&bar);
             }
-            if (i < r.n) load_x<N>(L, r.order ? r.order[i] - L.order_base : i, x);
-            // the barrier that also publishes the rows stored by threads themselves; every
-            // thread learns whether all copies landed
-            const bool staged = __syncthreads_and(umma::mbar_wait(&bar, phase, kStageWaitPolls));
-            phase ^= 1u;
-            if (!staged) {
-                // the copies did not land: record it, give them a second bounded wait, and
-                // leave this CTA's systems unsolved
-                if (L.fault && tid == 0) *reinterpret_cast<volatile unsigned*>(L.fault) = 1u;
-                umma::mbar_wait(&bar, phase ^ 1u, kStageWaitPolls);
-                return;
-            }
-        } else if (r.order == nullptr && L.p_layout == GSB_AOS && L.p_off == nullptr) {
-            stage_aos<NP, RS, kThreads>(rows, L.P + base * NP, r.n - base, tid);
-        } else if (i < r.n) {
+            __syncthreads();
+            if (i >= r.n) return;
             const int64_t idx = r.order ? r.order[i] - L.order_base : i;
-            if (L.p_layout == GSB_SOA) {
-#pragma unroll 4
-                for (int k = 0; k < NP; ++k) prow[k] = __ldg(L.P + (int64_t)k * L.nsys + idx);
-            } else {
-                const double* pb = param_block(L, idx, NP);
-#pragma unroll 4
-                for (int k = 0; k < NP; ++k) prow[k] = __ldg(pb + k);
-            }
-        }
-        if constexpr (!kBulk) __syncthreads();
-        if (i >= r.n) return;
-        const int64_t idx = r.order ? r.order[i] - L.order_base : i;
-        Fam fam{prow};
-        if constexpr (SH > 0) fam.a = smem;
-        double* xb = x_block(L, idx, N);
-        if constexpr (!kBulk) load_x<N>(L, idx, x);
-        Solver<Fam, F, Mixed, PlainRef, Qr> sv(fam, m, o, N >= 6 ? prow + NP : nullptr);
-        double gr;
-        DevStatus s = sv.solve(x, gr);
-#pragma unroll
-        for (int k = 0; k < N; ++k) {
-            if (L.x_layout == GSB_SOA) L.X[(int64_t)k * L.nsys + idx] = x[k];
-            else xb[k] = x[k];
-        }
-        if (L.s_kind == GSB_STATUS64) store_status(L.S, idx, s, gr);
-        else reinterpret_cast<unsigned char*>(L.S)[idx] = (unsigned char)s.code;
-        if (L.tally) tally_code(L.tally, s.code);
-    });
+            double x[N];
+            load_x<N>(L, idx, x);
+            double gr;
+            const DevStatus st = solve_one<Fam, F, Mixed, PlainRef, Qr>(m, o, smem, prow, x, gr);
+            store_one<N>(L, idx, x, st, gr);
+            if (L.tally) tally_code(L.tally, st.code);
+        });
+    }
 }
 
 
@@ -494,10 +585,12 @@ struct KernelEntry {
 };
 
 template <class Fam, bool F, bool Mixed, bool PlainRef> KernelEntry* entry() {
+    // the kernels of a family with aligned rows work warp by warp over the whole batch: launch
+    // the resident CTAs only
     static KernelEntry e{newton_kernel<Fam, F, Mixed, PlainRef, false>,
                          newton_kernel<Fam, F, Mixed, PlainRef, true>,
                          ((SharedLen<Fam>::value + 1) / 2) * 2 + kThreads * newton_row_stride<Fam>(),
-                         kThreads, {}};
+                         kThreads, {}, PairsOf<Fam>::value};
     return &e;
 }
 

@@ -37,6 +37,14 @@ struct DevState {
     int slow_steps;
 };
 
+// What a step that took the common course (Backtracking's first trial accepted at alpha = 1)
+// already formed for the stopping tests that follow it, with their own operands and operations:
+// record's rate, the norm of the new iterate, and the quotient th / (1 - th) of the rate test.
+struct StepSpec {
+    bool valid;
+    double rate, xnorm, q;
+};
+
 // record(status, info), src/base/status.jl:245-262.
 __device__ __forceinline__ void record(DevStatus& s, const StepInfo& i) {
     s.rate = s.stepnorm > 0.0 ? __ddiv_rn(i.stepnorm, s.stepnorm) : kNaN;
@@ -776,6 +784,47 @@ template <class Fam, bool F, bool Mixed, bool PlainRef = false, bool Qr = false>
         return 2.0 * s;
     }
 
+    // Backtracking's common course, taken without a branch on the way: its first trial at
+    // alpha = 1 with the exact slope (the plain step's ExactStep, phi'(0) = -2 phi0), the trial's
+    // merit, |d| and, for the stopping tests after the step, the norm of the trial iterate, the
+    // rate against the previous step and the rate test's quotient, all formed side by side; then
+    // the conditions under which globalize (below) takes that trial as a SUCCESS at alpha = 1,
+    // tested together. True: the step is done (x, Fx, merit, info and sp are the bits globalize
+    // and the loop's own tests would give). False: nothing is written, and globalize runs.
+    __device__ __forceinline__ bool first_trial_accepted(double (&x)[N], double (&Fx)[M],
+                                                         const double (&d)[N], double& merit,
+                                                         StepInfo& info, double prev_stepnorm,
+                                                         double rate_k, StepSpec& sp) const {
+        const double phi0 = merit;
+        double xt[N], Ft[M];
+        const double pa = trial(x, d, 1.0, xt, Ft);
+        const double dn2 = norm2<F, N>(d);
+        const double xn2 = norm2<F, N>(xt);
+        const double dn = sqrt(dn2);
+        const double rate = prev_stepnorm > 0.0 ? __ddiv_rn(dn, prev_stepnorm) : kNaN;
+        const double th = jmax(rate, rate_k);
+        const double q = __ddiv_rn(th, __dsub_rn(1.0, th));
+        const double d0 = -2.0 * phi0;
+        const double tau = jmax(__dmul_rn(4.0 * kEps, fabs(phi0)), 4.0 * 4.9406564584124654e-324);
+        const double demand = __dmul_rn(m.bt_c1, d0);  // (c1 * alpha) * d0 at alpha = 1
+        const double dphi = __dsub_rn(pa, phi0);
+        const bool ok = isfin(dn2) && dn2 >= double(N) * kFloatmin  // rnorm(d) is sqrt(dn2)
+                        && isfin(phi0) && isfin(d0) && d0 < 0.0     // the search starts
+                        && !(tau > fabs(d0))                         // at alpha = 1
+                        && dphi <= jmin(0.0, __dadd_rn(demand, tau)) // Armijo holds
+                        && isfin(pa) && dphi < -tau;                 // and it is a SUCCESS
+        if (!ok) return false;
+#pragma unroll
+        for (int i = 0; i < N; ++i) x[i] = xt[i];
+#pragma unroll
+        for (int i = 0; i < M; ++i) Fx[i] = Ft[i];
+        merit = pa;
+        info = {SUCCESS, sqrt(pa), dn, 0, false, false, false};
+        const bool xr = isfin(xn2) && xn2 >= double(N) * kFloatmin;
+        sp = {true, rate, xr ? sqrt(xn2) : rnorm<F, N>(xt), q};
+        return true;
+    }
+
     // globalize!! for Static (src/globalization/linefunction.jl:114-131) and globalize_merit!!
     // with the Backtracking search (linefunction.jl:159-199, linesearch.jl:154-171,
     // backtracking.jl:62-132).
@@ -955,7 +1004,9 @@ template <class Fam, bool F, bool Mixed, bool PlainRef = false, bool Qr = false>
     }
 
     // The plain step (TF = T), src/nonlinear/newton.jl:1679-1688.
-    __device__ void step_plain(DevState& st, double (&x)[N], double (&Fx)[M], StepInfo& info) const {
+    __device__ void step_plain(DevState& st, double (&x)[N], double (&Fx)[M], StepInfo& info,
+                               double prev_stepnorm = 0.0, double rate_k = kNaN,
+                               StepSpec* sp = nullptr) const {
         if constexpr (kDeferGr) {
             // the gradient ratio is formed after the last step (stashed_grad_ratio)
             JS js;
@@ -1002,6 +1053,14 @@ template <class Fam, bool F, bool Mixed, bool PlainRef = false, bool Qr = false>
                     for (int i = 0; i < N; ++i) d[i] = -d[i];
                 }
                 unpark_x(x);
+                if constexpr (!PlainRef) {
+                    if (sp != nullptr && m.globalization == GSB_BACKTRACKING &&
+                        first_trial_accepted(x, Fx, d, merit, info, prev_stepnorm, rate_k, *sp)) {
+                        st.merit = merit;
+                        st.fnorm = info.fnorm;
+                        return;
+                    }
+                }
                 globalize(x, Fx, d, !PlainRef, merit, info);
             }
             st.merit = merit;
@@ -1232,9 +1291,22 @@ template <class Fam, bool F, bool Mixed, bool PlainRef = false, bool Qr = false>
         while (true) {
             const double rate_k = s.rate;
             StepInfo info;
+            StepSpec sp;
+            sp.valid = false;
             if (Mixed) step_mixed(st, x, Fx, info);
-            else step_plain(st, x, Fx, info);
-            record(s, info);
+            else step_plain(st, x, Fx, info, s.stepnorm, rate_k, &sp);
+            if (sp.valid) {
+                // record(s, info) with the rate the step formed from the same operands
+                s.rate = sp.rate;
+                s.code = info.code;
+                s.iterations += 1;
+                s.fnorm = info.fnorm;
+                s.stepnorm = info.stepnorm;
+                s.step_failures += info.failures;
+                s.promoted = s.promoted || info.promoted;
+            } else {
+                record(s, info);
+            }
             gr_out = st.gradratio;
             if (info.code == SINGULAR || info.code == NONFINITE || info.code == MAXITERS) return s;
             if (info.code == LINESEARCH_FAILED && info.stepnorm == 0.0) return s;
@@ -1246,13 +1318,15 @@ template <class Fam, bool F, bool Mixed, bool PlainRef = false, bool Qr = false>
                 return s;
             }
             const bool steptested = !(info.code == STALLED || info.limited);
-            const double xnorm = steptested ? rnorm<F, N>(x) : kNaN;
+            const double xnorm = steptested ? (sp.valid ? sp.xnorm : rnorm<F, N>(x)) : kNaN;
             bool contracted = false;
             if (!info.shortened && o.rate_test && s.iterations >= o.min_iterations) {
                 double th = jmax(s.rate, rate_k);
-                if (s.stepnorm > 0.0 && th < 1.0)
-                    contracted = __dmul_rn(__ddiv_rn(th, __dsub_rn(1.0, th)), s.stepnorm) <=
+                if (s.stepnorm > 0.0 && th < 1.0) {
+                    const double q = sp.valid ? sp.q : __ddiv_rn(th, __dsub_rn(1.0, th));
+                    contracted = __dmul_rn(q, s.stepnorm) <=
                                  __dmul_rn(o.kappa, jmax(o.x_abstol, __dmul_rn(o.x_reltol, xnorm)));
+                }
             }
             bool stepc = false;
             if (steptested && s.iterations >= o.min_iterations) {

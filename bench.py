@@ -162,16 +162,12 @@ def fp_peaks():
     return out
 
 
-def profile_traffic():
-    """DRAM bytes per launch of the plain kernel from the committed ncu summary, if present."""
-    path = os.path.join(ROOT, "profiles", "newton_cubic8_fp64.md")
-    if not os.path.exists(path):
-        return None
-    with open(path) as fh:
-        for line in fh:
-            if line.startswith("traffic_bytes_per_launch_full:"):
-                return float(line.split(":", 1)[1])
-    return None
+# DRAM bytes per launch of the plain n = 8 kernel (dram__bytes_read.sum + dram__bytes_write.sum)
+# from one ncu capture of 262,144 systems, scaled by 4 to the 1,048,576-system launch (traffic grows
+# with the systems): the capture and its command are in profiles/newton_cubic8_fp64.md. A figure
+# of a capture, not of this run: the line labels it so.
+TRAFFIC_PER_LAUNCH = 189.75e6 * 4
+TRAFFIC_SOURCE = "ncu capture (profiles/newton_cubic8_fp64.md), 262,144 systems scaled x4"
 
 
 # ─── clocks ──────────────────────────────────────────────────────────────────────────────────
@@ -421,19 +417,30 @@ def main():
         return max_over_ranks(e0.elapsed_time(e1) / steps)
 
     # kernel-only time of one launch (no copy), for the roofline
-    def kernel_ms(m, reps=5):
-        ts = []
-        for _ in range(reps):
-            X.copy_(X0)
-            torch.cuda.synchronize(dev)
-            a = torch.cuda.Event(enable_timing=True)
-            b = torch.cuda.Event(enable_timing=True)
-            a.record(stream)
-            G.solve_batch(X, S, prob, m, ps, options=opts)
-            b.record(stream)
-            torch.cuda.synchronize(dev)
-            ts.append(a.elapsed_time(b))
-        return statistics.median(ts)
+    def kernel_ms(m, reps=8):
+        """The kernel alone: `reps` launches through the C-ABI queued back to back on the stream
+        (each on its own copy of the start iterates, made beforehand), between two events, so
+        that no host work sits between the launches; the mean per launch."""
+        lib = G.load_library()
+        from gsb200 import batch as B
+
+        Xs = [X0.clone() for _ in range(reps)]
+        gm, go = B._abi_of(m), B._abi_of(opts)
+        gp = prob.to_abi(None)
+        st = ctypes.c_void_p(stream.cuda_stream)
+        torch.cuda.synchronize(dev)
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for Xr in Xs:
+            rc = lib.gsb_solve_batch(ctypes.byref(gp), ctypes.byref(gm), ctypes.byref(go),
+                                     Xr.data_ptr(), 0, S.data_ptr(), 0, P.data_ptr(), 0, None, 0,
+                                     nsys, st, None)
+            assert rc == 0, rc
+        b.record(stream)
+        torch.cuda.synchronize(dev)
+        assert lib.gsb_synchronize(st) == 0
+        return a.elapsed_time(b) / reps
 
     with Clocks(local) as clk:
         ms_plain = timed(plain, args.steps, args.warmup)
@@ -484,10 +491,11 @@ def main():
     t_flops = flops / (peaks["fp64"] * 1e12)
     achieved_gbs = bytes_total / (kms * 1e-3) / 1e9
     achieved_tf = flops / (kms * 1e-3) / 1e12
-    traffic = profile_traffic()
+    traffic = TRAFFIC_PER_LAUNCH if nsys == NSYS else None
     if t_bytes >= t_flops:
         roof = {"bound": "hbm", "achieved": achieved_gbs, "peak": hbm_peak, "unit": "GB/s",
                 "frac": achieved_gbs / hbm_peak, "traffic": traffic,
+                "traffic_source": TRAFFIC_SOURCE,
                 "peak_source": hbm_src}
     else:
         roof = {"bound": "fp64", "achieved": achieved_tf, "peak": peaks["fp64"],

@@ -298,7 +298,10 @@ int oracle_standard_cell(int32_t number, const double* x0, int32_t column, int32
     go.rate_test = 1;
     Opts o = to_opts(&go);
     Meth m;
+    // columns of test/verification/standard_reference.csv: 0 "Newton Static LU",
+    // 1 "Newton Backtracking LU", 2 "Newton Backtracking QR"
     m.glob = column == 0 ? G_STATIC : G_BACKTRACKING;
+    m.qr = column == 2;
     int n = -1;
     auto run = [&](auto prob) {
         using P = decltype(prob);

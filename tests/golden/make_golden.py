@@ -1,11 +1,12 @@
 """Generates tests/golden/standard_newton_lu_f64.json from the reference's golden table.
 
-Run in the container that holds the reference (it reads GeometricSolvers.jl's
-test/verification/standard_reference.csv, path given as the first argument or the default
-below). It keeps the Float64 rows of the columns "Newton Static LU" and "Newton Backtracking LU"
-(code, iterations, f_evals, fnorm and the unstable/platform flags) and adds each cell's start,
-restated from test/helpers/standard_problems.jl:386-424 (u0, and 10 u0 and 100 u0 where they
-differ from an earlier start, test/helpers/standard_problems.jl:44-52).
+python tests/golden/make_golden.py <path of GeometricSolvers.jl's
+    test/verification/standard_reference.csv>
+
+It keeps the Float64 rows of the columns in COLUMNS (code, iterations, f_evals, fnorm and the
+unstable/platform flags) and adds each cell's start, restated from
+test/helpers/standard_problems.jl:386-424 (u0, and 10 u0 and 100 u0 where they differ from an
+earlier start, test/helpers/standard_problems.jl:44-52).
 """
 
 import csv
@@ -14,7 +15,8 @@ import os
 import sys
 from fractions import Fraction
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference/test/verification/standard_reference.csv"
+COLUMNS = ("Newton Static LU", "Newton Backtracking LU", "Newton Backtracking QR",
+           "Newton DogLeg LU", "Newton reuse 3 Backtracking LU")
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "standard_newton_lu_f64.json")
 
 
@@ -59,18 +61,20 @@ def starts(number):
 
 
 def main():
+    if len(sys.argv) != 2:
+        sys.exit(__doc__)
     rows = {}
-    with open(REF) as fh:
+    with open(sys.argv[1]) as fh:
         for r in csv.DictReader(fh):
             if r["eltype"] != "Float64":
                 continue
-            if r["column"] not in ("Newton Static LU", "Newton Backtracking LU"):
+            if r["column"] not in COLUMNS:
                 continue
             rows[(int(r["problem"]), r["start"], r["column"])] = r
     cells = []
     for number in range(1, 24):
         for label, x0 in starts(number):
-            for column in ("Newton Static LU", "Newton Backtracking LU"):
+            for column in COLUMNS:
                 r = rows[(number, label, column)]
                 cells.append({
                     "problem": number, "start": label, "x0": x0, "column": column,
@@ -78,7 +82,7 @@ def main():
                     "f_evals": int(r["f_evals"]), "fnorm": float(r["fnorm"]),
                     "unstable": r["unstable"] == "true", "platform": r["platform"] == "true",
                 })
-    assert len(cells) == 134, len(cells)
+    assert len(cells) == 67 * len(COLUMNS), len(cells)
     with open(OUT, "w") as fh:
         json.dump({"source": "test/verification/standard_reference.csv", "cells": cells}, fh, indent=1)
     print(f"wrote {len(cells)} cells to {OUT}")

@@ -1,8 +1,9 @@
 """The oracle pinned to the reference's own golden table and test assertions (CPU only).
 
 Pins (file:line within GeometricSolvers.jl):
-  test/verification/standard_reference.csv: Float64 rows of "Newton Static LU" and
-      "Newton Backtracking LU", compared as test/helpers/standard_cells.jl:377-399 compares them
+  test/verification/standard_reference.csv: Float64 rows of "Newton Static LU",
+      "Newton Backtracking LU" and "Newton Backtracking QR", compared as
+      test/helpers/standard_cells.jl:377-399 compares them
       (code exact, iterations within 1 on rows not flagged unstable/platform);
   test/nonlinear/batched.jl:461-499 (six outcomes), :263-397 (exact dyadic root, singular start);
   test/nonlinear/refinement.jl:466-632 (A_MOD, A_ILL) and :686-725 (Check 1);
@@ -28,9 +29,15 @@ def _cells():
         return json.load(fh)["cells"]
 
 
-@pytest.mark.parametrize("cell", _cells(), ids=lambda c: f"p{c['problem']}-{c['start']}-{c['column'].split()[1]}")
+# the golden table's columns the oracle restates, by its column index
+COLUMNS = {"Newton Static LU": 0, "Newton Backtracking LU": 1, "Newton Backtracking QR": 2}
+
+
+@pytest.mark.parametrize("cell", [c for c in _cells() if c["column"] in COLUMNS],
+                         ids=lambda c: f"p{c['problem']}-{c['start']}-" + "".join(
+                             w[0] for w in c["column"].split()[1:]))
 def test_standard_table(cell, oracle):
-    col = 0 if cell["column"] == "Newton Static LU" else 1
+    col = COLUMNS[cell["column"]]
     x, st, f_evals, _ = oracle.standard_cell(cell["problem"], np.array(cell["x0"]), col, 200)
     if cell["unstable"] or cell["platform"]:
         # the reference compares such a cell only for its presence

@@ -521,9 +521,16 @@ def main():
             O.solve_batch(prob, plain, X0_h[:sample].copy(), P_h[:sample], opts, nthreads=ntall)
             t_tot += time.perf_counter() - t0
             reps += 1
+        # one host thread on a smaller sample of the same batch
+        s1 = 32768
+        t0 = time.perf_counter()
+        O.solve_batch(prob, plain, X0_h[:s1].copy(), P_h[:s1], opts, nthreads=1)
+        t1 = time.perf_counter() - t0
         cpu = {"value": sample * reps / t_tot, "unit": "systems/s", "cores": ntall, "kind": "port",
                "sample": f"{reps} x {sample} of the {nsys} systems, plain FP64, "
-                         f"{ntall} threads, {t_tot:.1f} s"}
+                         f"{ntall} threads, {t_tot:.1f} s",
+               "value_1_thread": s1 / t1,
+               "sample_1_thread": f"{s1} of the {nsys} systems, plain FP64, 1 thread, {t1:.2f} s"}
 
     line = {
         "metric": METRIC, "value": value, "unit": "systems/s", "n_gpus": world,
@@ -1022,11 +1029,46 @@ def run_workload(args):
                 forms[name] = {"systems_per_s": float(np.sum(ok)) / (ms * 1e-3), "ms_per_step": ms,
                                "solved": int(np.sum(ok)), "fp64_oracle_max_rel_err": float(err.max()),
                                "table": tables[name]}
+            # the baseline of the comparison: plain FP64 with one ordinary launch per size
+            # bucket (each bucket a uniform batch of its own, laid out beforehand; no graph, no
+            # persistent kernels, each call waiting for its kernel as solve_batch! does)
+            buckets = []
+            for n in (2, 3, 4, 6, 8, 12, 16, 24, 32):
+                sel = np.flatnonzero(sizes_h == n)
+                if sel.size == 0:
+                    continue
+                xi = xoff_h[sel][:, None] + np.arange(n)[None, :]
+                pi = poff_h[sel][:, None] + np.arange(n * n + n)[None, :]
+                x0n = torch.tensor(X0_h[xi], device=dev)
+                buckets.append((n, sel, xi, x0n, torch.empty_like(x0n),
+                                torch.tensor(P_h[pi], device=dev), G.status_buffer(sel.size),
+                                G.NonlinearProblem(G.CubicAffine(n))))
+
+            def per_bucket():
+                for n, sel, xi, x0n, xn, pn, sn, pb in buckets:
+                    xn.copy_(x0n)
+                    G.solve_batch(xn, sn, pb, plain, G.PerSystem(pn), options=opts)
+
+            ms_b = _events_ms(per_bucket, args.steps, args.warmup, stream)
+            per_bucket()
+            okb = np.zeros(nsys, dtype=bool)
+            errb = np.zeros(nsys)
+            for n, sel, xi, x0n, xn, pn, sn, pb in buckets:
+                stb = G.statuses(sn)
+                errb[sel] = rel_err(xn.cpu().numpy(), xo_all[xi])
+                okb[sel] = (stb["code"] == so_all["code"][sel]) & (errb[sel] <= REL_TOL)
+            forms["plain_fp64_per_bucket_launches"] = {
+                "systems_per_s": float(np.sum(okb)) / (ms_b * 1e-3), "ms_per_step": ms_b,
+                "solved": int(np.sum(okb)), "fp64_oracle_max_rel_err": float(errb.max()),
+                "launches": len(buckets)}
+            del buckets
         clocks = clk.summary()
-        chosen = max(forms, key=lambda k: forms[k]["systems_per_s"])
+        chosen = max(("plain_fp64", "fp32_lu_refinement"), key=lambda k: forms[k]["systems_per_s"])
         value = forms[chosen]["systems_per_s"]
         ms = forms[chosen]["ms_per_step"]
         forms["chosen_over_plain"] = value / forms["plain_fp64"]["systems_per_s"]
+        forms["chosen_over_per_bucket_launches"] = (
+            value / forms["plain_fp64_per_bucket_launches"]["systems_per_s"])
         m_ch = mixed if chosen == "fp32_lu_refinement" else plain
         kms = ms - _events_ms(lambda: X.copy_(X0), 20, 2, stream)
         kernel = "bucketing + 9 persistent bucket kernels (one CUDA graph)"

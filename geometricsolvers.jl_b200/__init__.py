@@ -14,6 +14,7 @@ from .api import (
     CubicAffine,
     Coupled2,
     DimensionMismatch,
+    DogLeg,
     ExpSum3,
     GaussNewton,
     Hetero6,

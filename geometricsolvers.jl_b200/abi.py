@@ -128,6 +128,9 @@ class GsbMethod(ctypes.Structure):
         ("regularization", ctypes.c_double),
         ("arithmetic", ctypes.c_int32),
         ("threads_per_system", ctypes.c_int32),
+        ("reuse", ctypes.c_int32),
+        ("pad_", ctypes.c_int32),
+        ("dogleg_radius", ctypes.c_double),
     ]
 
 
@@ -166,7 +169,7 @@ GSB_STATUS64, GSB_CODES = 0, 1
 GSB_LU, GSB_QR = 0, 1
 GSB_F64, GSB_F32 = 0, 1
 GSB_NO_REFINEMENT, GSB_REFINEMENT = 0, 1
-GSB_STATIC, GSB_BACKTRACKING, GSB_LEVENBERG_MARQUARDT = 0, 1, 2
+GSB_STATIC, GSB_BACKTRACKING, GSB_LEVENBERG_MARQUARDT, GSB_DOGLEG = 0, 1, 2, 3
 GSB_FUSED, GSB_UNFUSED = 0, 1
 
 # The symbols include/gsb.h declares (checked by the CPU tests against the built library).

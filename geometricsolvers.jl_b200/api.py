@@ -155,6 +155,22 @@ class Backtracking:
 
 
 @dataclass(frozen=True)
+class DogLeg:
+    """DogLeg(; radius = nothing), src/globalization/dogleg.jl:1-60: the trust-region
+    globalization on the dogleg curve (Procedure 4.1 of Pawlowski, Simonis, Walker and Shadid
+    2008). `radius` is the initial trust radius, positive and finite, clamped to [1e-6, 1e10];
+    None lets the first step set it from the first Newton (or Cauchy) step."""
+
+    radius: Optional[float] = None
+
+    def __post_init__(self):
+        if self.radius is not None:
+            if not (self.radius > 0 and math.isfinite(self.radius)):
+                raise ArgumentError("the radius of DogLeg must be positive and finite")
+            object.__setattr__(self, "radius", min(max(float(self.radius), 1e-6), 1e10))
+
+
+@dataclass(frozen=True)
 class LevenbergMarquardt:
     """LevenbergMarquardt(; μ₀, μ_min, μ_max, μ_decrease, μ_increase, ρ_accept, scaling),
     src/globalization/levenbergmarquardt.jl:48-98 (the stacked QR path, scaling = :none)."""
@@ -234,6 +250,8 @@ class Newton:
                 raise ArgumentError("Newton reuse must be ≥ 1 or nothing")
             if isinstance(self.globalization, LevenbergMarquardt):
                 raise ArgumentError("Newton with a LevenbergMarquardt globalization takes no reuse")
+            if isinstance(self.globalization, DogLeg):
+                raise ArgumentError("DogLeg takes no factor reuse")
         if isinstance(self.globalization, LevenbergMarquardt) and isinstance(self.refinement, Refinement):
             raise ArgumentError(
                 "Newton with a LevenbergMarquardt globalization takes no refinement: a refinement "
@@ -269,14 +287,16 @@ class Newton:
             if g.scaling != "none":
                 raise ArgumentError("the batch LevenbergMarquardt step takes scaling = :none")
             lm = g
+        elif isinstance(g, DogLeg):
+            m.globalization = abi.GSB_DOGLEG
         else:
             raise ArgumentError(f"unsupported globalization {g!r}")
         m.lm_mu0, m.lm_mu_min, m.lm_mu_max = lm.mu0, lm.mu_min, lm.mu_max
         m.lm_mu_decrease, m.lm_mu_increase, m.lm_rho_accept = lm.mu_decrease, lm.mu_increase, lm.rho_accept
         if self.regularization != 0.0:
             raise ArgumentError("the batch path takes regularization = 0")
-        if self.reuse is not None:
-            raise ArgumentError("the batch path takes no factor reuse")
+        m.reuse = 0 if self.reuse is None else int(self.reuse)
+        m.dogleg_radius = (g.radius or 0.0) if isinstance(g, DogLeg) else 0.0
         m.regularization = 0.0
         m.arithmetic = abi.GSB_FUSED if self.arithmetic == "fused" else abi.GSB_UNFUSED
         m.threads_per_system = 0 if self.threads_per_system is None else self.threads_per_system

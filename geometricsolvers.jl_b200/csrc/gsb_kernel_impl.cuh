@@ -158,7 +158,7 @@ __device__ __forceinline__ void status_words(const DevStatus& s, double gr, unsi
     w[5] = (unsigned long long)__double_as_longlong(kNaN);
     w[6] = (unsigned long long)__double_as_longlong(gr);
     w[7] = (unsigned long long)__double_as_longlong(s.rate);
-    w[8] = (unsigned long long)(s.contracted ? 1u : 0u);
+    w[8] = (unsigned long long)(s.contracted ? 1u : 0u) | ((unsigned long long)(s.reused ? 1u : 0u) << 8);
 }
 
 __device__ __forceinline__ void store_status(void* S, int64_t idx, const DevStatus& s, double gr) {
@@ -216,14 +216,14 @@ template <class Fam, bool Mixed> constexpr int min_blocks() {
 }
 
 // The Newton solve of one system by its thread, once its parameter row is staged.
-template <class Fam, bool F, bool Mixed, bool PlainRef, bool Qr>
+template <class Fam, bool F, bool Mixed, bool PlainRef, bool Qr, int Kind = kStepNewton>
 __device__ __forceinline__ DevStatus solve_one(const GsbMethod& m, const GsbOptions& o,
                                                const double* smem, double* prow,
                                                double (&x)[Fam::N], double& gr) {
     constexpr int N = Fam::N, NP = Fam::NP;
     Fam fam{prow};
     if constexpr (SharedLen<Fam>::value > 0) fam.a = smem;
-    Solver<Fam, F, Mixed, PlainRef, Qr> sv(fam, m, o, N >= 6 ? prow + NP : nullptr);
+    Solver<Fam, F, Mixed, PlainRef, Qr, Kind> sv(fam, m, o, N >= 6 ? prow + NP : nullptr);
     return sv.solve(x, gr);
 }
 
@@ -276,7 +276,8 @@ __device__ __forceinline__ void store_one(const Launch& L, int64_t idx, const do
     else reinterpret_cast<unsigned char*>(L.S)[idx] = (unsigned char)s.code;
 }
 
-template <class Fam, bool F, bool Mixed, bool PlainRef, bool Persistent, bool Qr = false>
+template <class Fam, bool F, bool Mixed, bool PlainRef, bool Persistent, bool Qr = false,
+          int Kind = kStepNewton>
 __global__ void __launch_bounds__(kThreads, (min_blocks<Fam, Mixed>())) newton_kernel(const __grid_constant__ GsbMethod m,
                                  const __grid_constant__ GsbOptions o,
                                  const __grid_constant__ Launch L) {
@@ -344,7 +345,7 @@ __global__ void __launch_bounds__(kThreads, (min_blocks<Fam, Mixed>())) newton_k
             __syncwarp();  // the lanes' own stores of their rows (SoA) before any read
             DevStatus st{};
             double gr = kNaN;
-            if (mine) st = solve_one<Fam, F, Mixed, PlainRef, Qr>(m, o, smem, prow, x, gr);
+            if (mine) st = solve_one<Fam, F, Mixed, PlainRef, Qr, Kind>(m, o, smem, prow, x, gr);
             __syncwarp();  // the rows are free again
             static_assert(RS >= 9 && RS >= N, "a warp's rows hold its 32 statuses and iterates");
             if (c * 32 + 32 <= r.n && r.order == nullptr && L.s_kind == GSB_STATUS64 &&
@@ -382,7 +383,7 @@ __global__ void __launch_bounds__(kThreads, (min_blocks<Fam, Mixed>())) newton_k
             double x[N];
             load_x<N>(L, idx, x);
             double gr;
-            const DevStatus st = solve_one<Fam, F, Mixed, PlainRef, Qr>(m, o, smem, prow, x, gr);
+            const DevStatus st = solve_one<Fam, F, Mixed, PlainRef, Qr, Kind>(m, o, smem, prow, x, gr);
             store_one<N>(L, idx, x, st, gr);
             if (L.tally) tally_code(L.tally, st.code);
         });
@@ -594,6 +595,16 @@ template <class Fam, bool F, bool Mixed, bool PlainRef> KernelEntry* entry() {
     return &e;
 }
 
+// The Float64 LU step with factor reuse (Kind = kStepReuse) or with the DogLeg trust region
+// (kStepDogLeg), no refinement.
+template <class Fam, bool F, int Kind> KernelEntry* kind_entry() {
+    static KernelEntry e{newton_kernel<Fam, F, false, false, false, false, Kind>,
+                         newton_kernel<Fam, F, false, false, true, false, Kind>,
+                         ((SharedLen<Fam>::value + 1) / 2) * 2 + kThreads * newton_row_stride<Fam>(),
+                         kThreads, {}, PairsOf<Fam>::value};
+    return &e;
+}
+
 // The plain step with the static QR factor (QRFactorization, Float64, no refinement).
 template <class Fam, bool F> KernelEntry* qr_entry() {
     static KernelEntry e{newton_kernel<Fam, F, false, false, false, true>,
@@ -655,6 +666,15 @@ template <class Fam> KernelEntry* pick(bool fused, bool mixed, bool refine) {
         return fused ? qr_entry<__VA_ARGS__, true>() : qr_entry<__VA_ARGS__, false>();        \
     }
 #define GSB_DECLARE_TEAM(NAME) KernelEntry* team_##NAME(int T, bool mixed)
+#define GSB_DECLARE_KIND(NAME) KernelEntry* kind_##NAME(bool fused, int kind)
+#define GSB_DEFINE_KIND(NAME, ...)                                                            \
+    KernelEntry* kind_##NAME(bool fused, int kind) {                                          \
+        if (kind == kStepReuse)                                                               \
+            return fused ? kind_entry<__VA_ARGS__, true, kStepReuse>()                        \
+                         : kind_entry<__VA_ARGS__, false, kStepReuse>();                      \
+        return fused ? kind_entry<__VA_ARGS__, true, kStepDogLeg>()                           \
+                     : kind_entry<__VA_ARGS__, false, kStepDogLeg>();                         \
+    }
 #define GSB_DEFINE_ENTRY(NAME, ...)                                          \
     KernelEntry* entry_##NAME(bool fused, bool mixed, bool refine) {         \
         return pick<__VA_ARGS__>(fused, mixed, refine);                      \

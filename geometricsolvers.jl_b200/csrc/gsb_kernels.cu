@@ -239,6 +239,13 @@ GSB_DECLARE_ENTRY(hetero6);
 GSB_DECLARE_ENTRY(coupled2);
 GSB_DECLARE_TEAM(cubic6);
 GSB_DECLARE_TEAM(cubic8);
+GSB_DECLARE_KIND(cubic2);
+GSB_DECLARE_KIND(cubic3);
+GSB_DECLARE_KIND(cubic4);
+GSB_DECLARE_KIND(cubic6);
+GSB_DECLARE_KIND(cubic8);
+GSB_DECLARE_KIND(hetero6);
+GSB_DECLARE_KIND(coupled2);
 KernelEntry* lm_expsum3_64(bool fused, bool mixed);
 KernelEntry* warp_cubic12(bool fused, bool mixed, bool refine, int T);
 KernelEntry* warp_cubic16(bool fused, bool mixed, bool refine, int T);
@@ -275,6 +282,26 @@ KernelEntry* select_qr_kernel(const GsbProblem* prob, bool fused, int T) {
         }
     case GSB_FAMILY_HETERO6: return qr_hetero6(fused);
     case GSB_FAMILY_COUPLED2: return qr_coupled2(fused);
+    default: return nullptr;
+    }
+}
+
+// The kernel of a step with factor reuse or with DogLeg: one thread per system, a Float64 LU
+// factor, no refinement, a per-system parameter block.
+KernelEntry* select_kind_kernel(const GsbProblem* prob, bool fused, int kind, int T) {
+    if (T > 1 || shared_matrix(prob)) return nullptr;
+    switch (prob->family) {
+    case GSB_FAMILY_CUBIC_AFFINE:
+        switch (prob->n) {
+        case 2: return kind_cubic2(fused, kind);
+        case 3: return kind_cubic3(fused, kind);
+        case 4: return kind_cubic4(fused, kind);
+        case 6: return kind_cubic6(fused, kind);
+        case 8: return kind_cubic8(fused, kind);
+        default: return nullptr;
+        }
+    case GSB_FAMILY_HETERO6: return kind_hetero6(fused, kind);
+    case GSB_FAMILY_COUPLED2: return kind_coupled2(fused, kind);
     default: return nullptr;
     }
 }
@@ -356,8 +383,16 @@ int check_method(const GsbMethod* m) {
         return set_err(GSB_ERR_ARGUMENT, "linsolve must be LU or QR");
     if (m->factor_precision != GSB_F64 && m->factor_precision != GSB_F32)
         return set_err(GSB_ERR_ARGUMENT, "factor precision must be F64 or F32");
-    if (m->globalization < GSB_STATIC || m->globalization > GSB_LEVENBERG_MARQUARDT)
+    if (m->globalization < GSB_STATIC || m->globalization > GSB_DOGLEG)
         return set_err(GSB_ERR_ARGUMENT, "unknown globalization");
+    if (m->reuse < 0) return set_err(GSB_ERR_ARGUMENT, "Newton reuse must be >= 1 or nothing (0)");
+    if (m->reuse > 0 && m->globalization == GSB_LEVENBERG_MARQUARDT)
+        return set_err(GSB_ERR_ARGUMENT,
+                       "Newton with a LevenbergMarquardt globalization takes no reuse");
+    if (m->reuse > 0 && m->globalization == GSB_DOGLEG)
+        return set_err(GSB_ERR_ARGUMENT, "DogLeg takes no factor reuse");
+    if (!(m->dogleg_radius >= 0.0 && isfinite(m->dogleg_radius)))
+        return set_err(GSB_ERR_ARGUMENT, "the radius of DogLeg must be positive and finite");
     if (m->globalization == GSB_STATIC && !(m->static_alpha > 0.0 && isfinite(m->static_alpha)))
         return set_err(GSB_ERR_ARGUMENT, "the step of Static must be positive and finite");
     if (m->globalization == GSB_BACKTRACKING &&
@@ -429,7 +464,16 @@ int select_entry(const GsbProblem* prob, const GsbMethod* method, KernelEntry** 
         if (lm)
             return set_err(GSB_ERR_UNSUPPORTED,
                            "LevenbergMarquardt batch kernel only for least-squares families");
-        if (method->linsolve == GSB_QR) {
+        if (method->reuse > 0 || method->globalization == GSB_DOGLEG) {
+            // factor reuse and DogLeg: the Float64 LU step without refinement
+            if (method->linsolve != GSB_LU || mixed || method->refinement == GSB_REFINEMENT)
+                return set_err(GSB_ERR_UNSUPPORTED,
+                               "the batch kernels with factor reuse or DogLeg take a Float64 "
+                               "LUFactorization and no refinement");
+            ke = select_kind_kernel(prob, fused,
+                                    method->reuse > 0 ? gsb::kStepReuse : gsb::kStepDogLeg,
+                                    method->threads_per_system);
+        } else if (method->linsolve == GSB_QR) {
             if (mixed || method->refinement == GSB_REFINEMENT)
                 return set_err(GSB_ERR_UNSUPPORTED,
                                "the QRFactorization batch kernel takes a Float64 factor and no "
@@ -975,6 +1019,8 @@ int gsb_solve_batch_uneven(const GsbMethod* method, const GsbOptions* opt, doubl
     if (int rc = check_method(method)) return rc;
     if (method->globalization == GSB_LEVENBERG_MARQUARDT || method->linsolve != GSB_LU)
         return set_err(GSB_ERR_UNSUPPORTED, "ragged batches run Newton with LUFactorization");
+    if (method->reuse > 0 || method->globalization == GSB_DOGLEG)
+        return set_err(GSB_ERR_UNSUPPORTED, "ragged batches take no factor reuse and no DogLeg");
     if (s_kind != GSB_STATUS64 && s_kind != GSB_CODES) return set_err(GSB_ERR_ARGUMENT, "s_kind");
     if (tally) std::memset(tally, 0, sizeof(*tally));
     if (nsys == 0) return 0;

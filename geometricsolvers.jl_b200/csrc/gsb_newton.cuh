@@ -29,13 +29,23 @@ struct DevStatus {
     bool promoted, stationary;
     double rate;
     bool contracted;
+    bool reused = false;  // the last step stepped along a factor an earlier step formed
 };
 
 struct DevState {
     double merit, fnorm, gradratio, jnorm;
     bool promoted;
     int slow_steps;
+    // FactorAge (src/nonlinear/newton.jl:621-625) of Newton(reuse = k): the age of the held
+    // factor, whether it is to be refreshed, whether the last step reused it
+    int age;
+    bool stalled, reused;
+    double radius;  // TrustRadius of DogLeg (newton.jl:637-640); 0 while unset
 };
+
+// The step of the Newton solve: the method's own (plain, or the mixed-precision step), the step
+// with factor reuse, or the DogLeg trust-region step.
+enum StepKind : int { kStepNewton = 0, kStepReuse = 1, kStepDogLeg = 2 };
 
 // What a step that took the common course (Backtracking's first trial accepted at alpha = 1)
 // already formed for the stopping tests that follow it, with their own operands and operations:
@@ -591,14 +601,16 @@ template <bool F, int N> struct LocalLU {
 // state in registers.
 // Qr selects the static Householder QR for the plain step's factor (QRFactorization with a
 // Float64 factor), else the pivoted LU.
-template <class Fam, bool F, bool Mixed, bool PlainRef = false, bool Qr = false> struct Solver {
+template <class Fam, bool F, bool Mixed, bool PlainRef = false, bool Qr = false,
+          int Kind = kStepNewton>
+struct Solver {
     static constexpr int N = Fam::N, M = Fam::M;
     using JS = typename Fam::JState;
     using A = Arith<F>;
     // The plain step's gradient ratio feeds only the status of a square system, which keeps the
     // last factorisation's; where the step parks its start iterate and residual (N >= 6, the
     // kernel's stash), the ratio is formed once, after the last step, instead of at every step.
-    static constexpr bool kDeferGr = (N >= 6) && !Fam::lsq && !Mixed;
+    static constexpr bool kDeferGr = (N >= 6) && !Fam::lsq && !Mixed && Kind == kStepNewton;
     const Fam& fam;
     const GsbMethod& m;
     const GsbOptions& o;
@@ -1210,6 +1222,208 @@ template <class Fam, bool F, bool Mixed, bool PlainRef = false, bool Qr = false>
         st.fnorm = info.fnorm;
     }
 
+    // newton_step!! with reuse = k (Float64 factor, no refinement), src/nonlinear/newton.jl:
+    // 1783-1820: while the held factor is younger than k steps and the last step did not stall,
+    // the step solves with it and searches along that direction with the measured slope; a
+    // search that fails without a step is taken again, in the same step, from a fresh factor at
+    // the same point, which the steps after it hold (reuse_result, :1811-1820).
+    __device__ void step_reuse(DevState& st, double (&x)[N], double (&Fx)[M], StepInfo& info,
+                               LocalLU<F, N>& held) const {
+        const int age_fresh = m.reuse == 1 ? 0 : 1;  // fresh_age, newton.jl:629
+        if (!(st.age == 0 || st.stalled)) {
+            const int age_next = st.age + 1 >= m.reuse ? 0 : st.age + 1;  // next_age, :632-633
+            double d[N];
+            held.ldiv(Fx, d);
+#pragma unroll
+            for (int i = 0; i < N; ++i) d[i] = -d[i];
+            double xr[N], Fr[M];
+#pragma unroll
+            for (int i = 0; i < N; ++i) xr[i] = x[i];
+#pragma unroll
+            for (int i = 0; i < M; ++i) Fr[i] = Fx[i];
+            double merit = st.merit;
+            StepInfo ri;
+            globalize(xr, Fr, d, false, merit, ri);  // newton_line with fresh = false
+            if (!(ri.code == LINESEARCH_FAILED && ri.stepnorm == 0.0)) {
+#pragma unroll
+                for (int i = 0; i < N; ++i) x[i] = xr[i];
+#pragma unroll
+                for (int i = 0; i < M; ++i) Fx[i] = Fr[i];
+                info = ri;
+                st.merit = merit;
+                st.fnorm = info.fnorm;
+                st.reused = true;
+                st.age = age_next;
+                st.stalled = ri.code == STALLED;
+                return;
+            }
+        }
+        // a fresh factor (newton_factor, newton_globalize) at x
+        const double fnorm = residual_norm(st, Fx);
+        JS js;
+        fam.jacobian(x, js);
+        double gr, jn;
+        grad_ratio_and_norm(js, Fx, fnorm, gr, jn);
+        held.factor(fam, js);
+        double merit = st.merit;
+        if (held.info > 0) {
+            info = {SINGULAR, rnorm<F, M>(Fx), 0.0, 0, false, false, false};
+        } else {
+            double d[N];
+            held.ldiv(Fx, d);
+#pragma unroll
+            for (int i = 0; i < N; ++i) d[i] = -d[i];
+            globalize(x, Fx, d, true, merit, info);
+        }
+        st.gradratio = gr;
+        st.jnorm = jn;
+        st.merit = merit;
+        st.fnorm = info.fnorm;
+        st.reused = false;
+        st.age = info.code == SINGULAR ? 0 : age_fresh;
+        st.stalled = info.code == STALLED;
+    }
+
+    // J' v as a left fold down each column (the product with the adjoint of the SMatrix).
+    __device__ __forceinline__ void jtmul(const JS& js, const double (&v)[M], double (&out)[N]) const {
+#pragma unroll
+        for (int j = 0; j < N; ++j) {
+            double t = A::mul(fam.J(js, 0, j), v[0]);
+#pragma unroll
+            for (int i = 1; i < M; ++i) t = A::madd(fam.J(js, i, j), v[i], t);
+            out[j] = t;
+        }
+    }
+
+    // newton_step!! with DogLeg, src/nonlinear/newton.jl:1725-1747: one Jacobian, one factor, the
+    // Newton direction (none when the factor fails or its norm is zero or not finite), then the
+    // trial loop of dogleg_step on the Jacobian, with the radius the state carries.
+    __device__ void step_dogleg(DevState& st, double (&x)[N], double (&Fx)[M], StepInfo& info) const {
+        const double fnorm = residual_norm(st, Fx);
+        JS js;
+        fam.jacobian(x, js);
+        double gr, jn;
+        grad_ratio_and_norm(js, Fx, fnorm, gr, jn);
+        double d[N];
+        bool newton = false;
+        {
+            LUFactor<F, N, double> fac;
+            fac.factor(fam, js);
+            if (fac.info == 0) {  // dogleg_direction, :1751-1756
+                fac.ldiv(Fx, d);
+#pragma unroll
+                for (int i = 0; i < N; ++i) d[i] = -d[i];
+                const double nd = rnorm<F, N>(d);
+                newton = isfin(nd) && nd != 0.0;
+            }
+        }
+        dogleg_step(js, x, Fx, d, newton, st.radius, info);
+        st.gradratio = gr;
+        st.jnorm = jn;
+        st.fnorm = info.fnorm;
+    }
+
+    // dogleg_step, src/globalization/dogleg.jl:113-215 (Procedure 4.1 of Pawlowski, Simonis,
+    // Walker and Shadid 2008): the Newton step inside the radius, else the Cauchy point cut to
+    // it, else the point of norm delta on the segment between them; a trial is accepted when
+    // pred = |F| - |F + J s| > 0 and ared = |F| - |F(x + s)| >= 1e-4 pred, with the radius
+    // rules of that procedure. The Cauchy direction comes from the unit residual.
+    __device__ void dogleg_step(const JS& js, double (&x)[N], double (&Fx)[M], const double (&sN)[N],
+                                bool newton, double& delta, StepInfo& info) const {
+        const double lo = 1e-6, hi = 1e10;
+        const double fnorm = rnorm<F, M>(Fx);
+        if (fnorm == 0.0) {
+            info = {SUCCESS, fnorm, 0.0, 0, false, false, false};
+            return;
+        }
+        const double nN = newton ? rnorm<F, N>(sN) : kInf;
+        const double inv_f = __ddiv_rn(1.0, fnorm);
+        double u[M], gh[N], Jg[M];
+#pragma unroll
+        for (int i = 0; i < M; ++i) u[i] = __dmul_rn(inv_f, Fx[i]);
+        jtmul(js, u, gh);
+        const double gnorm = rnorm<F, N>(gh);
+        const double inv_g = __ddiv_rn(1.0, gnorm);
+#pragma unroll
+        for (int j = 0; j < N; ++j) gh[j] = __dmul_rn(inv_g, gh[j]);
+        jmul(js, gh, Jg);
+        const double jnorm = rnorm<F, M>(Jg);
+        const bool cauchy = gnorm != 0.0 && isfin(gnorm) && jnorm != 0.0 && isfin(jnorm);
+        const double nC = __dmul_rn(fnorm, __ddiv_rn(__ddiv_rn(gnorm, jnorm), jnorm));
+        if (delta == 0.0 && (newton || cauchy)) {
+            const double n0 = newton ? nN : nC;
+            delta = n0 < lo ? 2.0 * lo : jmin(jmax(n0, lo), hi);
+        }
+        while (true) {
+            double sv[N];
+            bool boundary;
+            if (newton && nN <= delta) {
+#pragma unroll
+                for (int j = 0; j < N; ++j) sv[j] = sN[j];
+                boundary = nN >= delta;
+            } else if (!cauchy) {
+                info = {STALLED, fnorm, 0.0, 0, false, false, false};
+                return;
+            } else if (!newton || nC >= delta) {
+                const double a = -jmin(nC, delta);
+#pragma unroll
+                for (int j = 0; j < N; ++j) sv[j] = __dmul_rn(a, gh[j]);
+                boundary = nC >= delta;
+            } else {
+                double a[N], b[N];
+                const double ca = -__ddiv_rn(nC, delta);
+#pragma unroll
+                for (int j = 0; j < N; ++j) a[j] = __dmul_rn(ca, gh[j]);
+#pragma unroll
+                for (int j = 0; j < N; ++j) b[j] = A::madd(nC, gh[j], sN[j]);
+                const double inv_b = __ddiv_rn(1.0, rnorm<F, N>(b));
+#pragma unroll
+                for (int j = 0; j < N; ++j) b[j] = __dmul_rn(inv_b, b[j]);
+                double ab = A::mul(a[0], b[0]);
+#pragma unroll
+                for (int j = 1; j < N; ++j) ab = A::madd(a[j], b[j], ab);
+                const double c = __dsub_rn(1.0, norm2<F, N>(a));
+                const double ab2 = __dmul_rn(ab, ab);
+                const double t = __ddiv_rn(c, __dadd_rn(ab, __dsqrt_rn(__dadd_rn(ab2, c))));
+                const double dt = __dmul_rn(delta, t);
+#pragma unroll
+                for (int j = 0; j < N; ++j) sv[j] = A::madd(delta, a[j], A::mul(dt, b[j]));
+                boundary = true;
+            }
+            double Js[M], Fl[M];
+            jmul(js, sv, Js);
+#pragma unroll
+            for (int i = 0; i < M; ++i) Fl[i] = __dadd_rn(Fx[i], Js[i]);
+            const double pred = __dsub_rn(fnorm, rnorm<F, M>(Fl));
+            double xp[N], Fp[M];
+#pragma unroll
+            for (int j = 0; j < N; ++j) xp[j] = __dadd_rn(x[j], sv[j]);
+            fam.F(xp, Fp);
+            const double fnp = rnorm<F, M>(Fp);
+            const double ared = __dsub_rn(fnorm, fnp);
+            if (pred > 0.0 && ared >= __dmul_rn(1e-4, pred)) {
+                const bool limited = !(newton && nN <= delta);
+                const double rho = __ddiv_rn(ared, pred);
+                if (rho < 0.1)
+                    delta = nN < delta ? jmax(nN, lo) : jmax(__dmul_rn(0.25, delta), lo);
+                else if (rho > 0.75 && boundary)
+                    delta = jmin(__dmul_rn(4.0, delta), hi);
+                const double stepnorm = rnorm<F, N>(sv);
+#pragma unroll
+                for (int j = 0; j < N; ++j) x[j] = xp[j];
+#pragma unroll
+                for (int i = 0; i < M; ++i) Fx[i] = Fp[i];
+                info = {SUCCESS, fnp, stepnorm, 0, false, limited, false};
+                return;
+            }
+            if (delta == lo) {
+                info = {LINESEARCH_FAILED, fnorm, 0.0, 1, false, false, false};
+                return;
+            }
+            delta = jmax(__dmul_rn(0.25, delta), lo);
+        }
+    }
+
     __device__ __forceinline__ bool residual_converged(const DevStatus& s, double ftest,
                                                        double ftest0) const {
         if (!(s.iterations >= o.min_iterations)) return false;
@@ -1266,6 +1480,12 @@ template <class Fam, bool F, bool Mixed, bool PlainRef = false, bool Qr = false>
         st.jnorm = 0.0;
         st.promoted = false;
         st.slow_steps = 0;
+        st.age = 0;  // reset_rule: FactorAge(0, false, false), TrustRadius(radius0, radius0)
+        st.stalled = false;
+        st.reused = false;
+        st.radius = m.dogleg_radius;
+        // the factor that steps with reuse hold from one step to the next (thread-local memory)
+        typename std::conditional<Kind == kStepReuse, LocalLU<F, N>, char>::type held;
         DevStatus s;
         s.code = SUCCESS;
         s.iterations = 0;
@@ -1276,6 +1496,7 @@ template <class Fam, bool F, bool Mixed, bool PlainRef = false, bool Qr = false>
         s.stationary = false;
         s.rate = kNaN;
         s.contracted = false;
+        s.reused = false;
         gr_out = kNaN;
         if (!isfin(fnorm0)) {
             s.code = NONFINITE;
@@ -1293,7 +1514,9 @@ template <class Fam, bool F, bool Mixed, bool PlainRef = false, bool Qr = false>
             StepInfo info;
             StepSpec sp;
             sp.valid = false;
-            if (Mixed) step_mixed(st, x, Fx, info);
+            if constexpr (Kind == kStepReuse) step_reuse(st, x, Fx, info, held);
+            else if constexpr (Kind == kStepDogLeg) step_dogleg(st, x, Fx, info);
+            else if (Mixed) step_mixed(st, x, Fx, info);
             else step_plain(st, x, Fx, info, s.stepnorm, rate_k, &sp);
             if (sp.valid) {
                 // record(s, info) with the rate the step formed from the same operands
@@ -1308,6 +1531,12 @@ template <class Fam, bool F, bool Mixed, bool PlainRef = false, bool Qr = false>
                 record(s, info);
             }
             gr_out = st.gradratio;
+            if constexpr (Kind == kStepReuse) {
+                // observe_rate!! (newton.jl:1205-1210): a step along a reused factor at a rate
+                // >= 1 refreshes the factor at the next step (a NaN rate refreshes nothing)
+                if (st.reused && s.rate >= 1.0) st.stalled = true;
+                s.reused = st.reused;
+            }
             if (info.code == SINGULAR || info.code == NONFINITE || info.code == MAXITERS) return s;
             if (info.code == LINESEARCH_FAILED && info.stepnorm == 0.0) return s;
             double ft = o.norm == 1 ? rmaxnorm<M>(Fx) : s.fnorm;

@@ -31,7 +31,7 @@
 extern "C" {
 #endif
 
-#define GSB_ABI_VERSION 1
+#define GSB_ABI_VERSION 2
 
 #if defined(__GNUC__)
 #define GSB_API __attribute__((visibility("default")))
@@ -148,7 +148,8 @@ typedef enum { GSB_FUSED = 0, GSB_UNFUSED = 1 } GsbArithmetic;
 typedef enum {
     GSB_STATIC = 0,
     GSB_BACKTRACKING = 1,
-    GSB_LEVENBERG_MARQUARDT = 2
+    GSB_LEVENBERG_MARQUARDT = 2,
+    GSB_DOGLEG = 3
 } GsbGlobalization;
 
 /*
@@ -183,6 +184,11 @@ typedef struct {
     int32_t arithmetic;         /* GsbArithmetic */
     int32_t threads_per_system; /* lanes of a warp that share one system: 1, 2, 4, 8, 16 or 32;
                                    0 = the library's tuned choice for the family and size */
+    int32_t reuse;              /* Newton(reuse = k): k >= 1; 0 = nothing (a fresh factor at
+                                   every step) */
+    int32_t pad_;
+    double dogleg_radius;       /* DogLeg(radius): the initial trust radius, > 0; 0 = nothing
+                                   (the first step sets it) */
 } GsbMethod;
 
 /* The six counts of the count form, src/nonlinear/batched.jl:197-199, by GsbReturnCode. */

@@ -56,6 +56,8 @@ Meth to_meth(const GsbMethod* g) {
     m.mu_decrease = g->lm_mu_decrease;
     m.mu_increase = g->lm_mu_increase;
     m.rho_accept = g->lm_rho_accept;
+    m.reuse = g->reuse;
+    m.dl_radius = g->dogleg_radius;
     return m;
 }
 
@@ -299,9 +301,11 @@ int oracle_standard_cell(int32_t number, const double* x0, int32_t column, int32
     Opts o = to_opts(&go);
     Meth m;
     // columns of test/verification/standard_reference.csv: 0 "Newton Static LU",
-    // 1 "Newton Backtracking LU", 2 "Newton Backtracking QR"
-    m.glob = column == 0 ? G_STATIC : G_BACKTRACKING;
+    // 1 "Newton Backtracking LU", 2 "Newton Backtracking QR", 3 "Newton DogLeg LU",
+    // 4 "Newton reuse 3 Backtracking LU"
+    m.glob = column == 0 ? G_STATIC : column == 3 ? G_DOGLEG : G_BACKTRACKING;
     m.qr = column == 2;
+    m.reuse = column == 4 ? 3 : 0;
     int n = -1;
     auto run = [&](auto prob) {
         using P = decltype(prob);

@@ -20,7 +20,7 @@ struct Opts {
     bool roundoff, rate_test;
 };
 
-enum Glob : int { G_STATIC = 0, G_BACKTRACKING = 1, G_LM = 2 };
+enum Glob : int { G_STATIC = 0, G_BACKTRACKING = 1, G_LM = 2, G_DOGLEG = 3 };
 
 // The Newton method fields the batch path reads, src/nonlinear/newton.jl:138-250, with
 // Backtracking (src/globalization/backtracking.jl:28-48), Static (static.jl:8-20),
@@ -35,6 +35,8 @@ struct Meth {
     int bt_maxiter = 100;
     double mu0 = 1e-6, mu_min = 1e-15, mu_max = 1e12, mu_decrease = 1.0 / 3.0, mu_increase = 4.0,
            rho_accept = 0.0;
+    int reuse = 0;            // Newton(reuse = k), k >= 1; 0: nothing
+    double dl_radius = 0.0;   // DogLeg(radius); 0: nothing (the first step sets it)
 };
 
 // SolverStatus{Float64}, src/base/status.jl:101-117 (counts of calls are 0 for these methods).
@@ -66,6 +68,13 @@ struct Diag {
 // the damping (LM rule state), the line-search anchor merit, the residual norm, the
 // diagnostics, and the mixed-precision flags.
 struct State {
+    // FactorAge, src/nonlinear/newton.jl:621-625: the age of the held factor, whether the last
+    // step stalled (or stepped along a reused factor at a rate >= 1), whether it stepped along a
+    // factor an earlier step formed
+    int age = 0;
+    bool stalled = false, reused = false;
+    // TrustRadius, newton.jl:637-640: DogLeg's radius (0 while unset)
+    double radius = 0.0;
     double mu = kNaN;
     double merit = kNaN;  // NaN where the globalization carries `nothing`
     double fnorm = kNaN;
@@ -254,6 +263,7 @@ template <class P> struct Solver {
     const Meth& m;
     const Opts& o;
     long f_evals = 0, dual_evals = 0;
+    Factor<N, double> held;  // the factor a step with reuse formed, for the steps after it
 
     Solver(const P& prob_, const Meth& m_, const Opts& o_) : prob(prob_), m(m_), o(o_) {}
 
@@ -753,8 +763,177 @@ template <class P> struct Solver {
 
     void step(State& st, double* x, double* Fx, StepInfo& info) {
         if (m.glob == G_LM) step_lm(st, x, Fx, info);
+        else if (m.glob == G_DOGLEG) step_dogleg(st, x, Fx, info);
+        else if (m.reuse > 0) step_reuse(st, x, Fx, info);
         else if (m.f32) step_mixed(st, x, Fx, info);
         else step_plain(st, x, Fx, info);
+    }
+
+    // newton_step!! with reuse = k (Float64 factor, no refinement), src/nonlinear/newton.jl:
+    // 1783-1820: while the held factor is younger than k steps and the last step did not stall,
+    // the step solves with it and searches along that direction with the measured slope; a
+    // search that fails without a step is taken again, in the same step, from a fresh factor at
+    // the same point. The rule state after the step follows reuse_result (:1811-1820).
+    void step_reuse(State& st, double* x, double* Fx, StepInfo& info) {
+        const int age_fresh = m.reuse == 1 ? 0 : 1;  // fresh_age, newton.jl:629
+        if (!(st.age == 0 || st.stalled)) {
+            const int age_next = st.age + 1 >= m.reuse ? 0 : st.age + 1;  // next_age, :632-633
+            double d[N];
+            ldiv_same<N>(held, Fx, d);
+            for (int i = 0; i < N; ++i) d[i] = -d[i];
+            double xr[N], Fr[M];
+            std::memcpy(xr, x, sizeof(xr));
+            std::memcpy(Fr, Fx, sizeof(Fr));
+            double merit = st.merit;
+            StepInfo ri;
+            globalize(xr, Fr, d, false, merit, ri);  // newton_line with fresh = false
+            if (!(ri.code == LINESEARCH_FAILED && ri.stepnorm == 0.0)) {
+                std::memcpy(x, xr, sizeof(xr));
+                std::memcpy(Fx, Fr, sizeof(Fr));
+                info = ri;
+                st.merit = merit;
+                st.fnorm = info.fnorm;
+                st.reused = true;
+                st.age = ri.code == SINGULAR ? 0 : age_next;
+                st.stalled = ri.code != SINGULAR && ri.code == STALLED;
+                return;
+            }
+        }
+        // a fresh factor (newton_factor, newton_globalize), kept for the steps after this one
+        double fnorm = residual_norm(st, Fx);
+        double J[M * N];
+        jacobian(x, J);
+        Diag dg;
+        grad_ratio_and_norm(J, Fx, fnorm, dg.gradratio, dg.jnorm);
+        held.factor(J, m.qr);
+        double merit = st.merit;
+        if (held.info() > 0) {
+            info = {SINGULAR, rnorm(Fx, M), 0.0, 0, false, false, false};
+        } else {
+            double d[N];
+            ldiv_same<N>(held, Fx, d);
+            for (int i = 0; i < N; ++i) d[i] = -d[i];
+            globalize(x, Fx, d, true, merit, info);
+        }
+        st.diag = dg;
+        st.merit = merit;
+        st.fnorm = info.fnorm;
+        st.reused = false;
+        st.age = info.code == SINGULAR ? 0 : age_fresh;
+        st.stalled = info.code != SINGULAR && info.code == STALLED;
+    }
+
+    // newton_step!! with DogLeg, src/nonlinear/newton.jl:1725-1747: one Jacobian, one factor, the
+    // Newton direction (none when the factor fails or its norm is zero or not finite), then the
+    // trial loop of dogleg_step on the Jacobian.
+    void step_dogleg(State& st, double* x, double* Fx, StepInfo& info) {
+        double fnorm = residual_norm(st, Fx);
+        double J[M * N];
+        jacobian(x, J);
+        Diag dg;
+        grad_ratio_and_norm(J, Fx, fnorm, dg.gradratio, dg.jnorm);
+        Factor<N, double> fac;
+        fac.factor(J, m.qr);
+        double d[N];
+        bool newton = false;
+        if (fac.info() == 0) {  // dogleg_direction, :1751-1756
+            ldiv_same<N>(fac, Fx, d);
+            for (int i = 0; i < N; ++i) d[i] = -d[i];
+            const double nd = rnorm(d, N);
+            newton = std::isfinite(nd) && nd != 0.0;
+        }
+        dogleg_step(x, Fx, J, d, newton, st.radius, info);
+        st.diag = dg;
+        st.fnorm = info.fnorm;
+    }
+
+    // dogleg_step, src/globalization/dogleg.jl:113-215 (Procedure 4.1 of Pawlowski, Simonis,
+    // Walker and Shadid 2008): the Newton step inside the radius, else the Cauchy point cut to it,
+    // else the point of norm delta on the segment between them; a trial is accepted when
+    // pred = |F| - |F + J s| > 0 and ared = |F| - |F(x + s)| >= 1e-4 pred.
+    void dogleg_step(double* x, double* Fx, const double* J, const double* sN, bool newton,
+                     double& delta, StepInfo& info) {
+        const double lo = 1e-6, hi = 1e10;
+        const double fnorm = rnorm(Fx, M);
+        if (fnorm == 0.0) {
+            info = {SUCCESS, fnorm, 0.0, 0, false, false, false};
+            return;
+        }
+        const double nN = newton ? rnorm(sN, N) : HUGE_VAL;
+        const double inv_f = 1.0 / fnorm;
+        double u[M], gt[N], gh[N], Jg[M];
+        for (int i = 0; i < M; ++i) u[i] = inv_f * Fx[i];
+        for (int j = 0; j < N; ++j) {  // J' u, a left fold down each column
+            double t = J[j * M] * u[0];
+            for (int i = 1; i < M; ++i) t = t + J[i + j * M] * u[i];
+            gt[j] = t;
+        }
+        const double gnorm = rnorm(gt, N);
+        const double inv_g = 1.0 / gnorm;
+        for (int j = 0; j < N; ++j) gh[j] = inv_g * gt[j];
+        matvec(J, gh, Jg);
+        const double jnorm = rnorm(Jg, M);
+        const bool cauchy = gnorm != 0.0 && std::isfinite(gnorm) && jnorm != 0.0 &&
+                            std::isfinite(jnorm);
+        const double nC = fnorm * ((gnorm / jnorm) / jnorm);
+        if (delta == 0.0 && (newton || cauchy)) {
+            const double n0 = newton ? nN : nC;
+            delta = n0 < lo ? 2.0 * lo : jmin(jmax(n0, lo), hi);  // clamp, dogleg.jl:64
+        }
+        while (true) {
+            double s[N];
+            bool boundary;
+            if (newton && nN <= delta) {
+                std::memcpy(s, sN, sizeof(s));
+                boundary = nN >= delta;
+            } else if (!cauchy) {
+                info = {STALLED, fnorm, 0.0, 0, false, false, false};
+                return;
+            } else if (!newton || nC >= delta) {
+                const double a = -jmin(nC, delta);
+                for (int j = 0; j < N; ++j) s[j] = a * gh[j];
+                boundary = nC >= delta;
+            } else {
+                double a[N], b[N];
+                const double ca = -(nC / delta);
+                for (int j = 0; j < N; ++j) a[j] = ca * gh[j];
+                for (int j = 0; j < N; ++j) b[j] = 1.0 * sN[j] + nC * gh[j];
+                const double inv_b = 1.0 / rnorm(b, N);
+                for (int j = 0; j < N; ++j) b[j] = inv_b * b[j];
+                const double ab = rdot(a, b, N);
+                const double c = 1.0 - norm2(a, N);
+                const double ab2 = ab * ab;
+                const double t = c / (ab + std::sqrt(ab2 + c));
+                const double dt = delta * t;
+                for (int j = 0; j < N; ++j) s[j] = delta * a[j] + dt * b[j];
+                boundary = true;
+            }
+            double Js[M], Flin[M];
+            matvec(J, s, Js);
+            for (int i = 0; i < M; ++i) Flin[i] = 1.0 * Fx[i] + 1.0 * Js[i];
+            const double pred = fnorm - rnorm(Flin, M);
+            double xp[N], Fp[M];
+            for (int j = 0; j < N; ++j) xp[j] = x[j] + 1.0 * s[j];
+            F(xp, Fp);
+            const double fnp = rnorm(Fp, M);
+            const double ared = fnorm - fnp;
+            if (pred > 0.0 && ared >= 1e-4 * pred) {
+                const bool limited = !(newton && nN <= delta);
+                const double rho = ared / pred;
+                if (rho < 0.1) delta = nN < delta ? jmax(nN, lo) : jmax(0.25 * delta, lo);
+                else if (rho > 0.75 && boundary) delta = jmin(4.0 * delta, hi);
+                const double stepnorm = rnorm(s, N);
+                std::memcpy(x, xp, sizeof(xp));
+                std::memcpy(Fx, Fp, sizeof(Fp));
+                info = {SUCCESS, fnp, stepnorm, 0, false, limited, false};
+                return;
+            }
+            if (delta == lo) {
+                info = {LINESEARCH_FAILED, fnorm, 0.0, 1, false, false, false};
+                return;
+            }
+            delta = jmax(0.25 * delta, lo);
+        }
     }
 
     // stationary_converged, src/nonlinear/solver.jl:148-158.
@@ -776,12 +955,14 @@ template <class P> struct Solver {
 
     // finish!! = newton_finish!!: the diagnostics of the last factorisation into the status.
     // src/nonlinear/newton.jl:1165-1184.
-    static Status finish(const State& st, const Status& s) {
+    // newton_finish!!, src/nonlinear/newton.jl:1169-1191: the diagnostics of the last
+    // factorisation and, under reuse, whether the last step stepped along a reused factor.
+    Status finish(const State& st, const Status& s) const {
         Status r = s;
         r.rank = st.diag.rank;
         r.nullnorm = st.diag.nullnorm;
         r.gradratio = st.diag.gradratio;
-        r.reused = false;
+        r.reused = m.reuse > 0 && st.reused && s.iterations > 0;
         return r;
     }
 
@@ -801,6 +982,10 @@ template <class P> struct Solver {
         st.promoted = false;
         st.slow_steps = 0;
         st.diag = Diag();
+        st.age = 0;                 // reset_rule: FactorAge(0, false, false)
+        st.stalled = false;
+        st.reused = false;
+        st.radius = m.dl_radius;    // reset_rule: TrustRadius(radius0, radius0)
         Status s0;
         s0.code = SUCCESS;
         s0.fnorm = fnorm0;
@@ -818,6 +1003,9 @@ template <class P> struct Solver {
             StepInfo info;
             step(st, x, Fx, info);
             status = record(status, info);
+            // observe_rate!!, newton.jl:1205-1210: a step along a reused factor at a rate >= 1
+            // refreshes the factor at the next step (a NaN rate refreshes nothing)
+            if (m.reuse > 0 && st.reused && status.rate >= 1.0) st.stalled = true;
             State st_step = st;
             if (info.code == SINGULAR || info.code == NONFINITE || info.code == MAXITERS)
                 return finish(st, status);

@@ -21,7 +21,7 @@ def test_header_and_exports(gsb):
     lib = gsb.load_library()
     for name in names:
         assert hasattr(lib, name), name
-    assert lib.gsb_abi_version() == 1
+    assert lib.gsb_abi_version() == 2
 
 
 def test_status_layout(gsb):

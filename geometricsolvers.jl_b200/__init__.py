@@ -38,6 +38,7 @@ from .api import (
     statuses,
 )
 from .batch import (batch_summary, ragged_offsets, solve_batch, solve_batch_host,
+                    solve_batch_summary,
                     solve_batch_uneven)
 from . import tune, warmstart
 from .warmstart import MlpWarmStart

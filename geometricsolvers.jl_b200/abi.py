@@ -181,6 +181,7 @@ EXPORTED_SYMBOLS = (
     "gsb_default_method",
     "gsb_solve_batch",
     "gsb_batch_summary",
+    "gsb_solve_batch_summary",
     "gsb_synchronize",
     "gsb_solve_batch_counts_noalloc",
     "gsb_uneven_sizes",
@@ -227,6 +228,12 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.gsb_solve_batch.restype = ctypes.c_int
     lib.gsb_batch_summary.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, P(GsbSummary)]
     lib.gsb_batch_summary.restype = ctypes.c_int
+    lib.gsb_solve_batch_summary.argtypes = [
+        P(GsbProblem), P(GsbMethod), P(GsbOptions),
+        ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
+        ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_void_p, P(GsbSummary),
+    ]
+    lib.gsb_solve_batch_summary.restype = ctypes.c_int
     lib.gsb_synchronize.argtypes = [ctypes.c_void_p]
     lib.gsb_synchronize.restype = ctypes.c_int
     lib.gsb_solve_batch_counts_noalloc.argtypes = [

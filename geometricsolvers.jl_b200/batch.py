@@ -109,7 +109,7 @@ def _shared_matrix(fam, A, device):
 
 
 def solve_batch(X, S, prob=None, method=None, p=None, *, order=None, options=None, stream=None,
-                **kwargs):
+                _summary=None, **kwargs):
     """Solve every system of X in place (see the module docstring). X is an (nsys, n) float64
     CUDA tensor (Vector{SVector}: one row per system) or SoA of an (n, nsys) tensor; S is a
     (nsys, 72) uint8 tensor of statuses (``status_buffer``). `order` is a permutation of
@@ -191,17 +191,46 @@ def solve_batch(X, S, prob=None, method=None, p=None, *, order=None, options=Non
     on_dev = torch.cuda.current_device() == Xt.device.index
     with contextlib.nullcontext() if on_dev else torch.cuda.device(Xt.device):
         st = ctypes.c_void_p(stream.cuda_stream)
-        rc = lib.gsb_solve_batch(
-            ctypes.byref(gp), ctypes.byref(gm), ctypes.byref(go), Xt.data_ptr(), x_layout,
-            S_buf.data_ptr(), s_kind, Pt.data_ptr(), p_layout,
-            None if order_t is None else order_t.data_ptr(), 0, nsys, st,
-            ctypes.byref(tally) if counts_form else None,
-        )
+        if _summary is not None:
+            rc = lib.gsb_solve_batch_summary(
+                ctypes.byref(gp), ctypes.byref(gm), ctypes.byref(go), Xt.data_ptr(), x_layout,
+                S_buf.data_ptr(), Pt.data_ptr(), p_layout,
+                None if order_t is None else order_t.data_ptr(), 0, nsys, st,
+                ctypes.byref(_summary))
+        else:
+            rc = lib.gsb_solve_batch(
+                ctypes.byref(gp), ctypes.byref(gm), ctypes.byref(go), Xt.data_ptr(), x_layout,
+                S_buf.data_ptr(), s_kind, Pt.data_ptr(), p_layout,
+                None if order_t is None else order_t.data_ptr(), 0, nsys, st,
+                ctypes.byref(tally) if counts_form else None,
+            )
         _raise_for(rc, lib)
         _raise_for(lib.gsb_synchronize(st), lib)
     if counts_form:
         return ReturnCodeCounts(*[int(c) for c in tally.counts])
     return S
+
+
+def solve_batch_summary(X, S, prob, method, p=None, *, order=None, options=None, stream=None,
+                        **kwargs):
+    """solve_batch(X, S, prob, method, p; ...) followed by batch_summary(S), with the summary
+    reduced by the solve's kernel as it closes the statuses (gsb_solve_batch_summary). Returns
+    (S, BatchSummary)."""
+    if isinstance(S, NonlinearProblem):
+        raise ArgumentError("solve_batch_summary takes a status vector S")
+    if nsys_of(X) == 0:
+        solve_batch(X, S, prob, method, p, order=order, options=options, stream=stream, **kwargs)
+        return S, BatchSummary(0.0, True, 0, 0, 0)
+    out = abi.GsbSummary()
+    solve_batch(X, S, prob, method, p, order=order, options=options, stream=stream,
+                _summary=out, **kwargs)
+    return S, BatchSummary(out.fnorm, bool(out.all_converged), int(out.failure_count),
+                           int(out.max_iterations), int(out.total_iterations))
+
+
+def nsys_of(X):
+    t = _tensor(X)
+    return t.shape[1] if isinstance(X, SoA) else t.shape[0]
 
 
 def batch_summary(S, stream=None) -> BatchSummary:

@@ -18,6 +18,62 @@ namespace gsb {
 
 constexpr int kThreads = 128;
 
+// batch_summary partials (src/nonlinear/batched.jl:63-89): Σ fnorm², max |fnorm|, failures,
+// max and Σ iterations, whether a fnorm was NaN.
+struct SummaryAcc {
+    double sumsq;
+    unsigned long long maxbits;  // bits of max |fnorm| (non-negative doubles order as integers)
+    unsigned long long failures;
+    unsigned long long total_iterations;
+    int max_iterations;
+    int nan_seen;
+};
+
+// One thread's share of a batch summary: the statuses it closed.
+struct SummaryPart {
+    double sumsq = 0.0;
+    unsigned long long maxbits = 0, failures = 0, iterations = 0;
+    int max_iterations = 0, nan = 0;
+
+    __device__ __forceinline__ void add(const DevStatus& s) {
+        sumsq = __fma_rn(s.fnorm, s.fnorm, sumsq);
+        const unsigned long long b = (unsigned long long)__double_as_longlong(fabs(s.fnorm));
+        maxbits = b > maxbits ? b : maxbits;
+        nan |= s.fnorm != s.fnorm;
+        failures += s.code != 0;
+        iterations += (unsigned long long)s.iterations;
+        max_iterations = s.iterations > max_iterations ? s.iterations : max_iterations;
+    }
+
+    // The parts of the active lanes of the warp, added up by the first of them into acc.
+    __device__ __forceinline__ void flush(SummaryAcc* acc) const {
+        const unsigned mask = __activemask();
+        const int lane = threadIdx.x & 31, leader = __ffs(mask) - 1;
+        double sq = 0.0;
+        unsigned long long mb = 0, fl = 0, it = 0;
+        int mx = 0, nn = 0;
+        for (int l = 0; l < 32; ++l) {
+            if (!(mask & (1u << l))) continue;
+            sq += __shfl_sync(mask, sumsq, l);
+            const unsigned long long b = __shfl_sync(mask, maxbits, l);
+            mb = b > mb ? b : mb;
+            fl += __shfl_sync(mask, failures, l);
+            it += __shfl_sync(mask, iterations, l);
+            const int m = __shfl_sync(mask, max_iterations, l);
+            mx = m > mx ? m : mx;
+            nn |= __shfl_sync(mask, nan, l);
+        }
+        if (lane == leader) {
+            atomicAdd(&acc->sumsq, sq);
+            atomicMax(&acc->maxbits, mb);
+            atomicAdd(&acc->failures, fl);
+            atomicAdd(&acc->total_iterations, it);
+            atomicMax(&acc->max_iterations, mx);
+            atomicOr(&acc->nan_seen, nn);
+        }
+    }
+};
+
 struct Launch {
     double* X;
     int x_layout;
@@ -45,6 +101,9 @@ struct Launch {
     // Set to nonzero when a wait for a staging copy ran out (the systems of that CTA are then
     // left unsolved); nullptr for none.
     unsigned* fault;
+    // The batch summary of the statuses the launch writes, accumulated as they close (the
+    // fused batch_summary); nullptr for none.
+    SummaryAcc* summary;
 };
 
 // The systems a launch solves: `n` entries of `order` (or 0 .. n-1 without one).
@@ -308,6 +367,7 @@ __global__ void __launch_bounds__(kThreads, (min_blocks<Fam, Mixed>())) newton_k
         __syncwarp();
         const Range r = launch_range(L);
         uint32_t phase = 0;
+        SummaryPart part;  // the lane's statuses, for a fused batch summary
         int64_t c = (int64_t)blockIdx.x * W + warp;
         while (true) {
             if constexpr (Persistent) {
@@ -358,8 +418,10 @@ __global__ void __launch_bounds__(kThreads, (min_blocks<Fam, Mixed>())) newton_k
                 store_one<N>(L, idx, x, st, gr);
             }
             if (L.tally && mine) tally_code(L.tally, st.code);
+            if (L.summary && mine) part.add(st);
             if constexpr (!Persistent) c += (int64_t)gridDim.x * W;
         }
+        if (L.summary) part.flush(L.summary);  // every lane leaves the loop together
         return;
     } else {
         for_each_chunk<Persistent>(L, kThreads, [&](int64_t base, const Range& r) {
@@ -386,6 +448,11 @@ __global__ void __launch_bounds__(kThreads, (min_blocks<Fam, Mixed>())) newton_k
             const DevStatus st = solve_one<Fam, F, Mixed, PlainRef, Qr, Kind>(m, o, smem, prow, x, gr);
             store_one<N>(L, idx, x, st, gr);
             if (L.tally) tally_code(L.tally, st.code);
+            if (L.summary) {
+                SummaryPart part;
+                part.add(st);
+                part.flush(L.summary);
+            }
         });
     }
 }
@@ -436,6 +503,11 @@ __global__ void __launch_bounds__(kThreads) team_kernel(const __grid_constant__ 
             if (L.s_kind == GSB_STATUS64) store_status(L.S, idx, s, gr);
             else reinterpret_cast<unsigned char*>(L.S)[idx] = (unsigned char)s.code;
             if (L.tally) tally_code(L.tally, s.code);
+            if (L.summary) {
+                SummaryPart part;
+                part.add(s);
+                part.flush(L.summary);
+            }
         }
     });
 }
@@ -505,6 +577,11 @@ __global__ void __launch_bounds__(kThreads, 2) lm_kernel(const __grid_constant__
             if (L.s_kind == GSB_STATUS64) store_status(L.S, idx, run.s, run.gr);
             else reinterpret_cast<unsigned char*>(L.S)[idx] = (unsigned char)run.s.code;
             if (L.tally) tally_code(L.tally, run.s.code);
+            if (L.summary) {
+                SummaryPart part;
+                part.add(run.s);
+                part.flush(L.summary);
+            }
             const long long q = (long long)atomicAdd(&next, 1ull);
             active = q < count;
             if (active) {
@@ -570,6 +647,11 @@ __global__ void __launch_bounds__(kThreads) warp_kernel(const __grid_constant__ 
             if (L.s_kind == GSB_STATUS64) store_status(L.S, idx, s, gr);
             else reinterpret_cast<unsigned char*>(L.S)[idx] = (unsigned char)s.code;
             if (L.tally) tally_code(L.tally, s.code);
+            if (L.summary) {
+                SummaryPart part;
+                part.add(s);
+                part.flush(L.summary);
+            }
         }
     });
 }

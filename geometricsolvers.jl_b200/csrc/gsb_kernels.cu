@@ -20,15 +20,6 @@
 
 namespace gsb {
 
-// batch_summary partials: Σ fnorm², max |fnorm|, failures, max and Σ iterations.
-struct SummaryAcc {
-    double sumsq;
-    unsigned long long maxbits;  // bits of max |fnorm| (non-negative doubles order as integers)
-    unsigned long long failures;
-    unsigned long long total_iterations;
-    int max_iterations;
-    int nan_seen;
-};
 
 __global__ void summary_kernel(const unsigned char* S, int64_t nsys, SummaryAcc* acc, int scale_e,
                                int pass) {
@@ -601,11 +592,12 @@ void gsb_default_method(GsbMethod* m) {
     m->threads_per_system = 0;
 }
 
-int gsb_solve_batch(const GsbProblem* prob, const GsbMethod* method, const GsbOptions* opt,
-                    double* X, int32_t x_layout, void* S, int32_t s_kind, const double* P,
-                    int32_t p_layout, const int64_t* order, int32_t order_base, int64_t nsys,
-                    void* stream, GsbTally* tally) {
-    g_err.clear();
+// gsb_solve_batch, and with `acc` (device memory, zeroed) the batch summary of the statuses
+// accumulated as the kernel closes them.
+int solve_batch_impl(const GsbProblem* prob, const GsbMethod* method, const GsbOptions* opt,
+                     double* X, int32_t x_layout, void* S, int32_t s_kind, const double* P,
+                     int32_t p_layout, const int64_t* order, int32_t order_base, int64_t nsys,
+                     void* stream, GsbTally* tally, SummaryAcc* acc) {
     if (!prob || !method || !opt) return set_err(GSB_ERR_ARGUMENT, "null problem, method or options");
     if (nsys < 0) return set_err(GSB_ERR_DIMENSION, "negative batch length");
     if (int rc = check_options(opt)) return rc;
@@ -658,6 +650,7 @@ int gsb_solve_batch(const GsbProblem* prob, const GsbMethod* method, const GsbOp
     Launch L{X, x_layout, S, s_kind, P, p_layout, order, order_base, nsys, prob->shared,
              ws ? ws->tally : nullptr};
     L.fault = fault_word();
+    L.summary = acc;
     int64_t blocks = 0;
     if (int rc = launch_blocks(ke, nsys, smem, &blocks)) return rc;
     ke->fn<<<(unsigned)blocks, kThreads, smem, st>>>(*method, *opt, L);
@@ -671,6 +664,54 @@ int gsb_solve_batch(const GsbProblem* prob, const GsbMethod* method, const GsbOp
         if (int rc = check_fault()) return rc;
         for (int c = 0; c < 6; ++c) tally->counts[c] = (int64_t)h[c];
     }
+    return 0;
+}
+
+int gsb_solve_batch(const GsbProblem* prob, const GsbMethod* method, const GsbOptions* opt,
+                    double* X, int32_t x_layout, void* S, int32_t s_kind, const double* P,
+                    int32_t p_layout, const int64_t* order, int32_t order_base, int64_t nsys,
+                    void* stream, GsbTally* tally) {
+    g_err.clear();
+    return solve_batch_impl(prob, method, opt, X, x_layout, S, s_kind, P, p_layout, order,
+                            order_base, nsys, stream, tally, nullptr);
+}
+
+// BatchSummary from the partials of a first pass (src/nonlinear/batched.jl:80-89): |F| is the
+// 2-norm of the per-system fnorms by rnorm's rule, so when the sum of squares left the normal
+// range a second pass over S sums the squares scaled by the largest |fnorm|'s exponent.
+int finish_summary(const SummaryAcc& h, const unsigned char* S, int64_t nsys, cudaStream_t st,
+                   Workspace* ws, GsbSummary* out) {
+    double s = h.sumsq;
+    double mx;
+    std::memcpy(&mx, &h.maxbits, sizeof(double));
+    double fnorm;
+    if (h.nan_seen) {
+        fnorm = __builtin_nan("");
+    } else if (std::isfinite(s) && s >= (double)nsys * 2.2250738585072014e-308) {
+        fnorm = std::sqrt(s);
+    } else if (mx == 0.0 || !std::isfinite(mx)) {
+        fnorm = mx;
+    } else {
+        int blocks = (int)((nsys + 255) / 256);
+        blocks = blocks > 1184 ? 1184 : blocks;
+        int e = std::ilogb(mx);
+        double zero = 0.0;
+        if (int rc = cuda_err(cudaMemcpyAsync(&ws->acc->sumsq, &zero, sizeof(double),
+                                              cudaMemcpyHostToDevice, st), "copy"))
+            return rc;
+        summary_kernel<<<blocks, 256, 0, st>>>(S, nsys, ws->acc, e, 1);
+        double s2 = 0;
+        if (int rc = cuda_err(cudaMemcpyAsync(&s2, &ws->acc->sumsq, sizeof(double),
+                                              cudaMemcpyDeviceToHost, st), "copy"))
+            return rc;
+        if (int rc = cuda_err(cudaStreamSynchronize(st), "sync")) return rc;
+        fnorm = std::ldexp(std::sqrt(s2), e);
+    }
+    out->fnorm = fnorm;
+    out->failure_count = (int64_t)h.failures;
+    out->all_converged = h.failures == 0;
+    out->max_iterations = h.max_iterations;
+    out->total_iterations = (int64_t)h.total_iterations;
     return 0;
 }
 
@@ -695,37 +736,36 @@ int gsb_batch_summary(const GsbStatus64* S, int64_t nsys, void* stream, GsbSumma
     if (int rc = cuda_err(cudaMemcpyAsync(&h, ws->acc, sizeof(h), cudaMemcpyDeviceToHost, st), "copy"))
         return rc;
     if (int rc = cuda_err(cudaStreamSynchronize(st), "sync")) return rc;
-    double s = h.sumsq;
-    double mx;
-    std::memcpy(&mx, &h.maxbits, sizeof(double));
-    double fnorm;
-    if (h.nan_seen) {
-        fnorm = __builtin_nan("");
-    } else if (std::isfinite(s) && s >= (double)nsys * 2.2250738585072014e-308) {
-        fnorm = std::sqrt(s);
-    } else if (mx == 0.0 || !std::isfinite(mx)) {
-        fnorm = mx;
-    } else {
-        int e = std::ilogb(mx);
-        double zero = 0.0;
-        if (int rc = cuda_err(cudaMemcpyAsync(&ws->acc->sumsq, &zero, sizeof(double),
-                                              cudaMemcpyHostToDevice, st), "copy"))
+    return finish_summary(h, reinterpret_cast<const unsigned char*>(S), nsys, st, ws, out);
+}
+
+int gsb_solve_batch_summary(const GsbProblem* prob, const GsbMethod* method, const GsbOptions* opt,
+                            double* X, int32_t x_layout, GsbStatus64* S, const double* P,
+                            int32_t p_layout, const int64_t* order, int32_t order_base,
+                            int64_t nsys, void* stream, GsbSummary* out) {
+    g_err.clear();
+    if (!out) return set_err(GSB_ERR_ARGUMENT, "null summary");
+    std::memset(out, 0, sizeof(*out));
+    if (nsys == 0) {
+        if (int rc = solve_batch_impl(prob, method, opt, X, x_layout, S, GSB_STATUS64, P, p_layout,
+                                      order, order_base, nsys, stream, nullptr, nullptr))
             return rc;
-        summary_kernel<<<blocks, 256, 0, st>>>(reinterpret_cast<const unsigned char*>(S), nsys,
-                                               ws->acc, e, 1);
-        double s2 = 0;
-        if (int rc = cuda_err(cudaMemcpyAsync(&s2, &ws->acc->sumsq, sizeof(double),
-                                              cudaMemcpyDeviceToHost, st), "copy"))
-            return rc;
-        if (int rc = cuda_err(cudaStreamSynchronize(st), "sync")) return rc;
-        fnorm = std::ldexp(std::sqrt(s2), e);
+        out->all_converged = 1;
+        return 0;
     }
-    out->fnorm = fnorm;
-    out->failure_count = (int64_t)h.failures;
-    out->all_converged = h.failures == 0;
-    out->max_iterations = h.max_iterations;
-    out->total_iterations = (int64_t)h.total_iterations;
-    return 0;
+    Workspace* ws = nullptr;
+    if (int rc = workspace(&ws)) return rc;
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    if (int rc = cuda_err(cudaMemsetAsync(ws->acc, 0, sizeof(SummaryAcc), st), "memset")) return rc;
+    if (int rc = solve_batch_impl(prob, method, opt, X, x_layout, S, GSB_STATUS64, P, p_layout,
+                                  order, order_base, nsys, stream, nullptr, ws->acc))
+        return rc;
+    SummaryAcc h{};
+    if (int rc = cuda_err(cudaMemcpyAsync(&h, ws->acc, sizeof(h), cudaMemcpyDeviceToHost, st), "copy"))
+        return rc;
+    if (int rc = cuda_err(cudaStreamSynchronize(st), "sync")) return rc;
+    if (int rc = check_fault()) return rc;
+    return finish_summary(h, reinterpret_cast<const unsigned char*>(S), nsys, st, ws, out);
 }
 
 int gsb_synchronize(void* stream) {

@@ -259,6 +259,19 @@ GSB_API int gsb_solve_batch(const GsbProblem* prob, const GsbMethod* method, con
  * Synchronises `stream`. */
 GSB_API int gsb_batch_summary(const GsbStatus64* S, int64_t nsys, void* stream, GsbSummary* out);
 
+/* solve_batch!(X, S, prob, method, p; order, options) followed by batch_summary(S) (src/nonlinear/
+ * batched.jl:257-287 and 80-89), with the summary's reduction fused into the solve: each warp
+ * adds up the statuses it closes (the sum of fnorm^2, the largest |fnorm|, the failures, the
+ * largest and the total iteration count) and adds its part to the call's accumulator once, so
+ * the statuses are not read back; only when the sum of squares leaves the normal range does a
+ * second pass over S take rnorm's scaled sum. S is GsbStatus64[nsys] (device); *out (host) is
+ * written; the call synchronises `stream`. Arguments and errors as gsb_solve_batch. */
+GSB_API int gsb_solve_batch_summary(const GsbProblem* prob, const GsbMethod* method,
+                                    const GsbOptions* opt, double* X, int32_t x_layout,
+                                    GsbStatus64* S, const double* P, int32_t p_layout,
+                                    const int64_t* order, int32_t order_base, int64_t nsys,
+                                    void* stream, GsbSummary* out);
+
 /* Wait for the work queued on `stream`. Returns GSB_ERR_CUDA if a batch kernel reported that a
  * bounded wait for its parameter staging copies ran out (its systems were then left unsolved; no
  * such wait is expected to run out). */

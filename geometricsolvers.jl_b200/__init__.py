@@ -32,6 +32,7 @@ from .api import (
     ReturnCodeCounts,
     SoA,
     Static,
+    Wood,
     gauss3_tableau,
     isconverged,
     status_buffer,

@@ -35,6 +35,8 @@ class Family(IntEnum):
     IRK3_HENON_HEILES = 3
     HETERO6 = 100
     COUPLED2 = 101
+    WOOD = 102
+    CUBIC_AFFINE_DUAL = 103
 
 
 class GsbStatus64(ctypes.Structure):

@@ -341,13 +341,21 @@ class Family:
 
 
 class CubicAffine(Family):
-    """F(x, p) = A x + 0.1 x.^3 - b with p = (A column-major n×n, b)."""
+    """F(x, p) = A x + 0.1 x.^3 - b with p = (A column-major n×n, b). jacobian = "rule" (the
+    default) takes the family's written-out Jacobian; jacobian = "dual" takes the device's
+    generic forward-mode dual pass over the residual (n in 2, 3, 4), the same bits."""
 
     family = abi.Family.CUBIC_AFFINE
 
-    def __init__(self, n: int):
+    def __init__(self, n: int, jacobian: str = "rule"):
         if not (1 <= n <= 32):
             raise ArgumentError(f"CubicAffine takes 1 ≤ n ≤ 32, got {n}")
+        if jacobian not in ("rule", "dual"):
+            raise ArgumentError("jacobian must be 'rule' or 'dual'")
+        if jacobian == "dual":
+            if not (2 <= n <= 4):
+                raise ArgumentError("the dual-pass CubicAffine takes n in 2, 3, 4")
+            self.family = abi.Family.CUBIC_AFFINE_DUAL
         self.n = self.m = n
 
     @property
@@ -418,6 +426,21 @@ class Coupled2(Family):
     @property
     def param_count(self):
         return 2
+
+
+class Wood(Family):
+    """Wood's function (problem 4 of test/helpers/standard_problems.jl) with the coupling weight
+    w of its second and fourth residuals (20.2 in the standard problem) per system, p = (w,). A
+    family given by its residual alone: the device takes its Jacobian and JVP from dual passes."""
+
+    family = abi.Family.WOOD
+
+    def __init__(self):
+        self.n = self.m = 4
+
+    @property
+    def param_count(self):
+        return 1
 
 
 class NonlinearProblem:

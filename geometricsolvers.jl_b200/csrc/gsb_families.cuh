@@ -10,6 +10,7 @@
 // family's parameter block.
 #pragma once
 
+#include "gsb_dual.cuh"
 #include "gsb_numerics.cuh"
 
 namespace gsb {
@@ -193,6 +194,90 @@ __device__ __forceinline__ void for_each_J(const Fam& fam, const typename Fam::J
 // holds the full matrix; its JVP is J(x) v as a left fold (src/ad/jvp.jl:88-91).
 template <int N_, int M_> struct FullJState {
     double J[M_ * N_];
+};
+
+// ─── a family given by its residual alone ───────────────────────────────────────────────────
+// Fn::eval<S>(fam, x, out) writes the residual for any scalar S with the operations of
+// gsb_dual.cuh; the family evaluates it on Real for F, on Dual<N> seeded with the identity for
+// the Jacobian (one N-partial pass, src/ad/forwarddiff_static.jl:50-65) and on Dual<1> seeded
+// with v for the JVP (src/ad/jvp.jl:96-107). Parameters (Fn::NP doubles per system) are read
+// from the system's shared-memory row with par(k).
+template <class Fn> struct DualFamily {
+    static constexpr int N = Fn::N, M = Fn::N, NP = Fn::NP;
+    static constexpr bool lsq = false;
+    const double* p;
+    using JState = FullJState<N, M>;
+    __device__ __forceinline__ double par(int k) const { return lds(smem_addr(p) + 8u * k); }
+    __device__ __forceinline__ void F(const double (&x)[N], double (&out)[M]) const {
+        Real xr[N], r[M];
+#pragma unroll
+        for (int i = 0; i < N; ++i) xr[i] = Real{x[i]};
+        Fn::eval(*this, xr, r);
+#pragma unroll
+        for (int i = 0; i < M; ++i) out[i] = r[i].v;
+    }
+    __device__ __forceinline__ void jacobian(const double (&x)[N], JState& js) const {
+        Dual<N> xd[N], rd[M];
+#pragma unroll
+        for (int j = 0; j < N; ++j) {
+            xd[j].v = x[j];
+#pragma unroll
+            for (int k = 0; k < N; ++k) xd[j].p[k] = k == j ? 1.0 : 0.0;
+        }
+        Fn::eval(*this, xd, rd);
+#pragma unroll
+        for (int j = 0; j < N; ++j)
+#pragma unroll
+            for (int i = 0; i < M; ++i) js.J[i + j * M] = rd[i].p[j];
+    }
+    __device__ __forceinline__ double J(const JState& js, int i, int k) const { return js.J[i + k * M]; }
+    __device__ __forceinline__ void jvp(const double (&x)[N], const double (&v)[N],
+                                        double (&out)[M]) const {
+        Dual<1> xd[N], rd[M];
+#pragma unroll
+        for (int j = 0; j < N; ++j) {
+            xd[j].v = x[j];
+            xd[j].p[0] = v[j];
+        }
+        Fn::eval(*this, xd, rd);
+#pragma unroll
+        for (int i = 0; i < M; ++i) out[i] = rd[i].p[0];
+    }
+};
+
+// The cubic-affine residual of CubicAffineT written as a template over its scalar: each row
+// fma(A_in, x_n, ... fma(A_i2, x_2, A_i1 x_1)), then fma(0.1, (x_i x_i) x_i, row) - b_i, the
+// same operations as the written-out family, whose Jacobian rule this family's dual pass checks.
+template <int N_> struct CubicAffineFn {
+    static constexpr int N = N_, NP = N_ * N_ + N_;
+    template <class Fam, class S>
+    __device__ __forceinline__ static void eval(const Fam& f, const S (&x)[N], S (&out)[N]) {
+#pragma unroll
+        for (int i = 0; i < N; ++i) {
+            S t = f.par(i) * x[0];
+#pragma unroll
+            for (int j = 1; j < N; ++j) t = fmac(f.par(i + j * N), x[j], t);
+            S c = x[i] * x[i] * x[i];
+            out[i] = fmac(0.1, c, t) - f.par(N * N + i);
+        }
+    }
+};
+
+// Wood's function (problem 4 of the reference's standard set, test/helpers/standard_problems.jl)
+// with the coupling weight of its second and fourth residuals (20.2 in the standard problem) as
+// the one parameter w of a system.
+struct WoodFn {
+    static constexpr int N = 4, NP = 1;
+    template <class Fam, class S>
+    __device__ __forceinline__ static void eval(const Fam& f, const S (&x)[4], S (&out)[4]) {
+        const double w = f.par(0);
+        const S t1 = x[1] - x[0] * x[0];
+        const S t2 = x[3] - x[2] * x[2];
+        out[0] = -200.0 * x[0] * t1 - (1.0 - x[0]);
+        out[1] = 200.0 * t1 + w * (x[1] - 1.0) + 19.8 * (x[3] - 1.0);
+        out[2] = -180.0 * x[2] * t2 - (1.0 - x[2]);
+        out[3] = 180.0 * t2 + w * (x[3] - 1.0) + 19.8 * (x[1] - 1.0);
+    }
 };
 
 // ─── test/nonlinear/batched.jl:54-90: the six-outcome residual, p = outcome 1..6 ───────────

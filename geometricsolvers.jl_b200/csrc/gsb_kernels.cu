@@ -202,6 +202,9 @@ int64_t param_count(const GsbProblem* p) {
     case GSB_FAMILY_IRK3_HENON_HEILES: return 4;
     case GSB_FAMILY_HETERO6: return 1;
     case GSB_FAMILY_COUPLED2: return 2;
+    case GSB_FAMILY_WOOD: return p->n == 4 ? 1 : GSB_ERR_ARGUMENT;
+    case GSB_FAMILY_CUBIC_AFFINE_DUAL:
+        return (p->n >= 2 && p->n <= 4) ? (int64_t)p->n * p->n + p->n : GSB_ERR_ARGUMENT;
     default: return GSB_ERR_ARGUMENT;
     }
 }
@@ -228,6 +231,10 @@ GSB_DECLARE_ENTRY(cubic6s);
 GSB_DECLARE_ENTRY(cubic8s);
 GSB_DECLARE_ENTRY(hetero6);
 GSB_DECLARE_ENTRY(coupled2);
+GSB_DECLARE_ENTRY(wood);
+GSB_DECLARE_ENTRY(cubicdual2);
+GSB_DECLARE_ENTRY(cubicdual3);
+GSB_DECLARE_ENTRY(cubicdual4);
 GSB_DECLARE_TEAM(cubic6);
 GSB_DECLARE_TEAM(cubic8);
 GSB_DECLARE_KIND(cubic2);
@@ -349,6 +356,14 @@ KernelEntry* select_kernel(const GsbProblem* prob, bool fused, bool mixed, bool 
         }
     case GSB_FAMILY_HETERO6: return entry_hetero6(fused, mixed, refine);
     case GSB_FAMILY_COUPLED2: return entry_coupled2(fused, mixed, refine);
+    case GSB_FAMILY_WOOD: return entry_wood(fused, mixed, refine);
+    case GSB_FAMILY_CUBIC_AFFINE_DUAL:
+        switch (prob->n) {
+        case 2: return entry_cubicdual2(fused, mixed, refine);
+        case 3: return entry_cubicdual3(fused, mixed, refine);
+        case 4: return entry_cubicdual4(fused, mixed, refine);
+        default: return nullptr;
+        }
     default: return nullptr;
     }
 }

@@ -118,7 +118,15 @@ typedef enum {
     GSB_FAMILY_IRK3_HENON_HEILES = 3,
     /* Test families of the reference's batch tests, with analytic Jacobians (prob.J). */
     GSB_FAMILY_HETERO6 = 100,  /* test/nonlinear/batched.jl:54-90; p = outcome 1..6; n = 2 */
-    GSB_FAMILY_COUPLED2 = 101  /* test/nonlinear/batched.jl:92-104; p = (p1, p2); n = 2 */
+    GSB_FAMILY_COUPLED2 = 101, /* test/nonlinear/batched.jl:92-104; p = (p1, p2); n = 2 */
+    /* Families given by their residual alone, their Jacobian and JVP from forward-mode dual
+     * passes on the device (src/ad/forwarddiff_static.jl:50-65, src/ad/jvp.jl:96-107):
+     * Wood's function (problem 4 of test/helpers/standard_problems.jl) with the coupling weight
+     * of its second and fourth residuals (20.2 there) as the one parameter, p = (w), n = 4; and
+     * the cubic-affine family of GSB_FAMILY_CUBIC_AFFINE (same p) with the dual pass in place of
+     * its written-out Jacobian, n in {2, 3, 4}. */
+    GSB_FAMILY_WOOD = 102,
+    GSB_FAMILY_CUBIC_AFFINE_DUAL = 103
 } GsbFamily;
 
 typedef struct {

@@ -147,6 +147,8 @@ int64_t param_count(int family, int n, int m) {
     case GSB_FAMILY_IRK3_HENON_HEILES: return 4;
     case GSB_FAMILY_HETERO6: return 1;
     case GSB_FAMILY_COUPLED2: return 2;
+    case GSB_FAMILY_WOOD: return 1;
+    case GSB_FAMILY_CUBIC_AFFINE_DUAL: return (int64_t)n * n + n;
     case FAM_QUADMOD2: return 6;
     case FAM_CUBICDIAG2: return 8;
     default: return -1;
@@ -265,6 +267,17 @@ int oracle_solve_batch(const GsbProblem* prob, const GsbMethod* method, const Gs
         run_batch<Coupled2>(b, m, o, 2, [](const double* p, const double*) { return Coupled2{p}; },
                             nt);
         return 0;
+    case GSB_FAMILY_WOOD:
+        if (n != 4) return GSB_ERR_UNSUPPORTED;
+        run_batch<Wood>(b, m, o, 1, [](const double* p, const double*) { return Wood{p}; }, nt);
+        return 0;
+    case GSB_FAMILY_CUBIC_AFFINE_DUAL:  // the oracle's cubic family already takes dual passes
+        switch (n) {
+        case 2: return run_cubic<2>(b, m, o, nt);
+        case 3: return run_cubic<3>(b, m, o, nt);
+        case 4: return run_cubic<4>(b, m, o, nt);
+        default: return GSB_ERR_UNSUPPORTED;
+        }
     case FAM_QUADMOD2:
         run_batch<QuadMod2>(b, m, o, 6, [](const double* p, const double*) { return QuadMod2{p}; },
                             nt);

@@ -59,6 +59,24 @@ template <int N_> struct CubicAffine {
     void J(const double*, double*) const {}
 };
 
+// ─── GSB_FAMILY_WOOD: Wood's function with the coupling weight w = p[0] ─────────────────────
+// Problem 4 of test/helpers/standard_problems.jl (w = 20.2 there), generic over double and Dual.
+struct Wood {
+    static constexpr int N = 4, M = 4;
+    static constexpr bool lsq = false, analytic_J = false;
+    const double* p;
+    template <class S> void F(const S* x, S* out) const {
+        const double w = p[0];
+        S t1 = x[1] - x[0] * x[0];
+        S t2 = x[3] - x[2] * x[2];
+        out[0] = -200.0 * x[0] * t1 - (1.0 - x[0]);
+        out[1] = 200.0 * t1 + w * (x[1] - 1.0) + 19.8 * (x[3] - 1.0);
+        out[2] = -180.0 * x[2] * t2 - (1.0 - x[2]);
+        out[3] = 180.0 * t2 + w * (x[3] - 1.0) + 19.8 * (x[1] - 1.0);
+    }
+    void J(const double*, double*) const {}
+};
+
 // ─── GSB_FAMILY_EXPSUM3_LSQ: r_i = a1 e^{-b1 t_i} + a2 e^{-b2 t_i} + a3 e^{-b3 t_i} - y_i ──────
 // x = (a1, b1, a2, b2, a3, b3), p = y (M values), t = the shared abscissae.
 template <int M_> struct ExpSum3 {

@@ -141,7 +141,8 @@ class GsbTally(ctypes.Structure):
 
 
 class GsbBucketConfig(ctypes.Structure):
-    _fields_ = [("threads_per_system", ctypes.c_int32), ("ctas_per_sm", ctypes.c_int32)]
+    _fields_ = [("threads_per_system", ctypes.c_int32), ("ctas_per_sm", ctypes.c_int32),
+                ("systems_per_cta", ctypes.c_int32), ("pad_", ctypes.c_int32)]
 
 
 GSB_UNEVEN_BUCKETS = 9

@@ -273,7 +273,9 @@ def solve_batch_uneven(X, S, sizes, P, method, *, x_off=None, p_off=None, table=
     packed float64 vector X and its parameter block (A column-major, then b) is P[p_off[s] :
     p_off[s] + n^2 + n]. S is a (nsys, 72) uint8 status tensor, or None for the count form (the
     six return-code counts are returned). `table` is a list of nine (threads_per_system,
-    ctas_per_sm) pairs, one per size (see ``tune.autotune_uneven``); None takes the defaults.
+    ctas_per_sm, systems_per_cta) triples (or pairs, systems_per_cta 0), one per size (see
+    ``tune.autotune_uneven``); None takes the table tuned on B200 for the method's form, which
+    the package carries, or the library's defaults where it has none.
     The offsets default to the back-to-back packing of ``ragged_offsets``."""
     import torch
 
@@ -325,12 +327,22 @@ def solve_batch_uneven(X, S, sizes, P, method, *, x_off=None, p_off=None, table=
                 f"status vector length {S.numel() // 72} does not match batch length {nsys}")
         S_buf = S
         s_kind = abi.GSB_STATUS64
+    if table is None:
+        from .tune import tuned_table
+
+        table = tuned_table(method)  # the committed table of the method's form, if any
     tab = None
     if table is not None:
         if len(table) != abi.GSB_UNEVEN_BUCKETS:
             raise ArgumentError(f"table takes {abi.GSB_UNEVEN_BUCKETS} entries")
-        tab = (abi.GsbBucketConfig * abi.GSB_UNEVEN_BUCKETS)(
-            *[abi.GsbBucketConfig(int(t), int(c)) for t, c in table])
+        rows = []
+        for t in table:
+            t = tuple(int(v) for v in t)
+            if len(t) not in (2, 3):
+                raise ArgumentError("a table entry is (threads_per_system, ctas_per_sm"
+                                    "[, systems_per_cta])")
+            rows.append(abi.GsbBucketConfig(*(t + (0,) * (3 - len(t)))))
+        tab = (abi.GsbBucketConfig * abi.GSB_UNEVEN_BUCKETS)(*rows)
     gm, go = method.to_abi(), opt.to_abi()
     if nsys == 0:
         return ReturnCodeCounts(0, 0, 0, 0, 0, 0) if counts_form else S

@@ -262,6 +262,20 @@ __device__ __forceinline__ void stage_aos(double* smem, const double* src, int64
     asm volatile("cp.async.wait_all;" ::: "memory");
 }
 
+// The same for a CTA of `nthreads` threads staging `rows` rows (the CTA size chosen at launch).
+template <int NP, int RS, class Place = IdentityPlace>
+__device__ __forceinline__ void stage_aos_rows(double* smem, const double* src, int64_t rows_left,
+                                               int rows, int tid, int nthreads,
+                                               Place place = Place()) {
+    const int total = (rows_left < rows ? (int)rows_left : rows) * NP;
+    for (int q = tid; q < total; q += nthreads) {
+        const int s = q / NP;
+        const unsigned dst = smem_addr(smem + s * RS + place(q - s * NP));
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(dst), "l"(src + q) : "memory");
+    }
+    asm volatile("cp.async.wait_all;" ::: "memory");
+}
+
 // Resident 128-thread blocks per SM that the register allocation must allow, by system size.
 // Measured on B200 for 1M systems: n = 4 runs 18-21% faster at 4 blocks (128 registers) than at
 // the allocator's own choice, n = 6 30% (plain, 4 blocks) and 20% (mixed, 3 blocks); n = 8 needs
@@ -595,11 +609,12 @@ __global__ void __launch_bounds__(kThreads, 2) lm_kernel(const __grid_constant__
     }
 }
 
-// The warp form (n = 12 ... 32): T lanes per system, kThreads / T systems per CTA. Each system's
-// shared memory holds its parameter block in the family's layout (SP doubles), then its N x LD
-// factor.
-template <class Fam> __host__ __device__ constexpr int warp_sys_stride() {
-    return ((Fam::SP + 1) / 2) * 2 + Fam::N * warp_ld(Fam::N);
+// The warp form (n = 12 ... 32): T lanes per system, blockDim.x / T systems per CTA (up to
+// kThreads / T; the launch chooses). Each system's shared memory holds its parameter block in
+// the family's layout (SP doubles), then its factor's part (the whole factor for teams of 16,
+// the two pivot-row buffers for teams of 32, whose rows live in the lanes' registers).
+template <class Fam, int T> __host__ __device__ constexpr int warp_sys_stride() {
+    return ((Fam::SP + 1) / 2) * 2 + warp_lu_doubles<Fam::N, T>();
 }
 
 // Parameter k of a system to its place in the family's shared-memory layout.
@@ -607,19 +622,36 @@ template <class Fam> struct WarpPlace {
     __device__ __forceinline__ int operator()(int k) const { return Fam::place(k); }
 };
 
+// Resident 128-thread blocks per SM that the warp kernel's register allocation must allow (0:
+// no bound). Measured on B200 (65,536 systems, 2 steps each): a team of 32 at n = 32 runs 1.74
+// ms at 3 blocks (168 registers, a few spilled) against 2.34 ms at the allocator's 179 registers
+// (2 blocks); n = 24 1.19 ms at 4 blocks (128 registers) against 1.24 ms. The 16-lane teams
+// (n = 12, 16; factor in shared memory) run fastest unbounded (94 registers); a 32-lane team at
+// n = 12 or 16 takes a minimum of one block, without which the allocator holds it to 96
+// registers and spills.
+template <class Fam, int T> constexpr int warp_min_blocks() {
+#ifdef GSB_WARP_MIN_BLOCKS
+    return GSB_WARP_MIN_BLOCKS;
+#else
+    return T != 32 ? 0 : Fam::N >= 32 ? 3 : Fam::N >= 24 ? 4 : 1;
+#endif
+}
+
 template <class Fam, int T, bool F, bool Mixed, bool PlainRef, bool Persistent>
-__global__ void __launch_bounds__(kThreads) warp_kernel(const __grid_constant__ GsbMethod m,
+__global__ void __launch_bounds__(kThreads, (warp_min_blocks<Fam, T>())) warp_kernel(const __grid_constant__ GsbMethod m,
                                  const __grid_constant__ GsbOptions o,
                                  const __grid_constant__ Launch L) {
     extern __shared__ double smem[];
-    constexpr int N = Fam::N, NP = Fam::NP, SPB = kThreads / T, SS = warp_sys_stride<Fam>();
+    constexpr int N = Fam::N, NP = Fam::NP, SS = warp_sys_stride<Fam, T>();
     const int tid = threadIdx.x;
     const int team = tid / T;
+    const int spb = (int)blockDim.x / T;
     double* sys = smem + team * SS;
-    for_each_chunk<Persistent>(L, SPB, [&](int64_t base, const Range& r) {
+    for_each_chunk<Persistent>(L, spb, [&](int64_t base, const Range& r) {
         const int64_t i = base + team;
         if (r.order == nullptr && L.p_layout == GSB_AOS && L.p_off == nullptr) {
-            stage_aos<NP, SS, SPB>(smem, L.P + base * NP, r.n - base, tid, WarpPlace<Fam>());
+            stage_aos_rows<NP, SS>(smem, L.P + base * NP, r.n - base, spb, tid, (int)blockDim.x,
+                                   WarpPlace<Fam>());
         } else if (i < r.n) {
             const int64_t idx = r.order ? r.order[i] - L.order_base : i;
             const double* pb = param_block(L, idx, NP);
@@ -665,6 +697,10 @@ struct KernelEntry {
     int systems_per_block;
     bool attr_set[64];
     bool resident = false;  // fn works through ranges of systems: launch the resident CTAs only
+    // The warp form takes its CTA size at launch: `lanes` threads and `sys_doubles` doubles of
+    // shared memory per system (0: the CTA size is fixed at kThreads).
+    int lanes = 0;
+    int sys_doubles = 0;
 };
 
 template <class Fam, bool F, bool Mixed, bool PlainRef> KernelEntry* entry() {
@@ -705,7 +741,8 @@ template <class Fam, bool F, bool Mixed> KernelEntry* lm_entry() {
 template <class Fam, int T, bool F, bool Mixed, bool PlainRef> KernelEntry* warp_entry() {
     static KernelEntry e{warp_kernel<Fam, T, F, Mixed, PlainRef, false>,
                          warp_kernel<Fam, T, F, Mixed, PlainRef, true>,
-                         (kThreads / T) * warp_sys_stride<Fam>(), kThreads / T, {}};
+                         (kThreads / T) * warp_sys_stride<Fam, T>(), kThreads / T, {}, false, T,
+                         warp_sys_stride<Fam, T>()};
     return &e;
 }
 

@@ -976,8 +976,9 @@ int uneven_streams(UnevenPlan& p) {
     return 0;
 }
 
-// The kernel of bucket b and its persistent grid; nullptr when the combination has no kernel.
-int uneven_entry(const UnevenKey& k, int b, int sms, KernelEntry** ke, unsigned* grid) {
+// The kernel of bucket b, its persistent grid and its CTA (threads, bytes of shared memory).
+int uneven_entry(const UnevenKey& k, int b, int sms, KernelEntry** ke, unsigned* grid,
+                 unsigned* threads, size_t* smem) {
     GsbProblem prob{};
     prob.family = GSB_FAMILY_CUBIC_AFFINE;
     prob.n = prob.m = kUnevenSizes[b];
@@ -989,20 +990,34 @@ int uneven_entry(const UnevenKey& k, int b, int sms, KernelEntry** ke, unsigned*
     if (!*ke) return set_err(GSB_ERR_UNSUPPORTED, "no kernel for bucket n = " +
                                                       std::to_string(kUnevenSizes[b]) +
                                                       " with these threads per system");
-    const size_t smem = (size_t)(*ke)->smem_doubles * sizeof(double);
-    int dev = 0;
-    if (int rc = cuda_err(cudaGetDevice(&dev), "cudaGetDevice")) return rc;
-    (void)dev;
+    *threads = kThreads;
+    *smem = (size_t)(*ke)->smem_doubles * sizeof(double);
+    const int spc = k.table[b].systems_per_cta;
+    if (spc != 0) {
+        // the warp form takes its CTA size at launch; the other forms have theirs fixed
+        const int lanes = (*ke)->lanes;
+        if (lanes == 0 || spc < 0 || spc * lanes > kThreads || (spc * lanes) % 32 != 0)
+            return set_err(GSB_ERR_ARGUMENT,
+                           "systems_per_cta of bucket n = " + std::to_string(kUnevenSizes[b]) +
+                               ": 0, or (for the warp form, n >= 12) a count whose CTA of "
+                               "systems_per_cta x threads_per_system lanes is a multiple of 32 "
+                               "and at most " + std::to_string(kThreads));
+        *threads = (unsigned)(spc * lanes);
+        *smem = (size_t)spc * (*ke)->sys_doubles * sizeof(double);
+    }
     if (!(*ke)->fn_persistent) return set_err(GSB_ERR_UNSUPPORTED, "no persistent bucket kernel");
-    // the persistent form of the bucket's kernel (set once per capture, which is rare)
+    // the persistent form of the bucket's kernel (set once per capture, which is rare); the
+    // attribute is the largest CTA the kernel takes, so that every CTA size fits under it
+    const size_t smem_max = (size_t)(*ke)->smem_doubles * sizeof(double);
     if (int rc = cuda_err(cudaFuncSetAttribute(reinterpret_cast<const void*>((*ke)->fn_persistent),
                                                cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               (int)smem), "cudaFuncSetAttribute"))
+                                               (int)std::max(smem_max, *smem)),
+                          "cudaFuncSetAttribute"))
         return rc;
     int occ = 0;
     if (int rc = cuda_err(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                              &occ, reinterpret_cast<const void*>((*ke)->fn_persistent), kThreads,
-                              smem),
+                              &occ, reinterpret_cast<const void*>((*ke)->fn_persistent),
+                              (int)*threads, *smem),
                           "occupancy"))
         return rc;
     if (occ < 1) return set_err(GSB_ERR_UNSUPPORTED, "a bucket kernel does not fit on an SM");
@@ -1017,9 +1032,10 @@ int uneven_capture(UnevenPlan& p, const UnevenKey& k, bool want_tally) {
     if (int rc = cuda_err(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "attr"))
         return rc;
     KernelEntry* ke[GSB_UNEVEN_BUCKETS];
-    unsigned grid[GSB_UNEVEN_BUCKETS];
+    unsigned grid[GSB_UNEVEN_BUCKETS], threads[GSB_UNEVEN_BUCKETS];
+    size_t smem[GSB_UNEVEN_BUCKETS];
     for (int b = 0; b < GSB_UNEVEN_BUCKETS; ++b)
-        if (int rc = uneven_entry(k, b, sms, &ke[b], &grid[b])) return rc;
+        if (int rc = uneven_entry(k, b, sms, &ke[b], &grid[b], &threads[b], &smem[b])) return rc;
     if (p.exec) {
         cudaGraphExecDestroy(p.exec);
         p.exec = nullptr;
@@ -1040,8 +1056,7 @@ int uneven_capture(UnevenPlan& p, const UnevenKey& k, bool want_tally) {
         Launch L{k.X, GSB_AOS, k.S, k.s_kind, k.P, GSB_AOS, p.list, 0, k.nsys, nullptr,
                  want_tally ? p.work->tally : nullptr, k.x_off, k.p_off, &p.work->queue[b],
                  &p.work->range[b][0], fault};
-        ke[b]->fn_persistent<<<grid[b], kThreads, (size_t)ke[b]->smem_doubles * sizeof(double), p.side[b]>>>(
-            k.m, k.o, L);
+        ke[b]->fn_persistent<<<grid[b], threads[b], smem[b], p.side[b]>>>(k.m, k.o, L);
         cudaEventRecord(p.join[b], p.side[b]);
         cudaStreamWaitEvent(p.cs, p.join[b], 0);
     }

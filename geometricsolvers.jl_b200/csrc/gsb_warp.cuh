@@ -15,6 +15,8 @@
 // oracle's exactly, as the one-thread kernels' do.
 #pragma once
 
+#include <type_traits>
+
 #include "../../include/gsb.h"
 #include "gsb_families.cuh"
 #include "gsb_newton.cuh"
@@ -261,9 +263,236 @@ template <int N, int T, bool F> struct WarpVec {
     }
 };
 
+// The pivot row of the warp factor in shared memory: written by the lane that holds it, read by
+// every lane of the team, pairs of entries as one 16-byte (Float64) or 8-byte (Float32) access.
+__device__ __forceinline__ void sts_one(unsigned a, double v) {
+    asm volatile("st.shared.f64 [%0], %1;" ::"r"(a), "d"(v) : "memory");
+}
+__device__ __forceinline__ void sts_one(unsigned a, float v) {
+    asm volatile("st.shared.f32 [%0], %1;" ::"r"(a), "f"(v) : "memory");
+}
+__device__ __forceinline__ void sts_pair(unsigned a, double v0, double v1) { sts2(a, v0, v1); }
+__device__ __forceinline__ void sts_pair(unsigned a, float v0, float v1) {
+    asm volatile("st.shared.v2.f32 [%0], {%1, %2};" ::"r"(a), "f"(v0), "f"(v1) : "memory");
+}
+__device__ __forceinline__ void lds_one(unsigned a, double& v) { v = lds(a); }
+__device__ __forceinline__ void lds_one(unsigned a, float& v) {
+    asm volatile("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(a));
+}
+__device__ __forceinline__ void lds_pair(unsigned a, double& v0, double& v1) { lds2(a, v0, v1); }
+__device__ __forceinline__ void lds_pair(unsigned a, float& v0, float& v1) {
+    asm volatile("ld.shared.v2.f32 {%0, %1}, [%2];" : "=f"(v0), "=f"(v1) : "r"(a));
+}
+
+// The pivoted LU of an N x N matrix held in registers: lane i < N keeps row i of the matrix it
+// was given, and the factor's row exchanges (lu.jl:24-64: the first largest |a_ik|, i >= k, a
+// NaN on the diagonal keeping k) move positions instead of rows. `pos` is the position the
+// lane's row holds after the exchanges so far; position k's lane writes its row into a shared
+// buffer at step k and the other lanes update their rows from it. Every entry goes through the
+// operations of the elimination with physical exchanges, in the same order, so the factor's
+// values, the pivot sequence and `info` are those of the reference's LU bit for bit. Row k of
+// the factor is the row of lane `owner` of lane k.
+//
+// The pivot search is a maximum over the team of a 64-bit key, the bits of |a_ik| plus one
+// (a NaN at position k counts as +Inf, one below never wins, a lane that holds no candidate has
+// key 0), then the smallest position among the lanes that hold it: three warp reductions and a
+// ballot in place of a butterfly of shuffles. Every member function is inlined, so that the
+// rows stay in registers.
+template <int N, int T, bool F, class TF> struct WarpRegLU {
+    // the fused factor divides by multiplying with pivot reciprocals (see LUFactor); in the
+    // back substitution that takes a division off each of the N sequential steps
+    static constexpr bool kRecip = F;
+    static constexpr int kBuf = ((N + 1) / 2) * 2 * (sizeof(double) / sizeof(TF));  // in TF
+    using A = Arith<F>;
+    TF* buf;  // two pivot-row buffers of kBuf entries, 16-byte aligned
+    TF r[N];  // the lane's row: multipliers left of its pivot column, then the U part
+    int pos;  // the row's position (-1 in a lane that holds no row)
+    int owner;  // in lane k < N: the lane whose row is row k of the factor
+    int info, e;
+
+    __device__ __forceinline__ unsigned slot(int k) const {
+        return smem_addr(buf) + (unsigned)(((k & 1) * kBuf) * sizeof(TF));
+    }
+
+    // Row k of the factor (from column k on) into buffer k & 1, by the lane that holds it, and
+    // back out in every lane
+    // entries K..N-1: one alone where K is odd, then pairs (even first index), then the last
+    template <int K> __device__ __forceinline__ void put_row(unsigned b) const {
+        constexpr int S = K + (K & 1);
+        if constexpr (K & 1) sts_one(b + K * (unsigned)sizeof(TF), r[K]);
+#pragma unroll
+        for (int j = S; j + 1 < N; j += 2) sts_pair(b + j * (unsigned)sizeof(TF), r[j], r[j + 1]);
+        if constexpr (S < N && ((N - S) & 1)) sts_one(b + (N - 1) * (unsigned)sizeof(TF), r[N - 1]);
+    }
+    template <int K> __device__ __forceinline__ void get_row(unsigned b, TF (&p)[N]) const {
+        constexpr int S = K + (K & 1);
+        if constexpr (K & 1) lds_one(b + K * (unsigned)sizeof(TF), p[K]);
+#pragma unroll
+        for (int j = S; j + 1 < N; j += 2) lds_pair(b + j * (unsigned)sizeof(TF), p[j], p[j + 1]);
+        if constexpr (S < N && ((N - S) & 1)) lds_one(b + (N - 1) * (unsigned)sizeof(TF), p[N - 1]);
+    }
+
+    // One step of the elimination: pivot search in column K, then the update of every row
+    // below position K.
+    template <int K> __device__ __forceinline__ void step(const Team<T>& tm) {
+        const int lane = tm.lane;
+        unsigned long long key = 0ull;
+        if (pos >= K) {
+            const double v = double(fabs(r[K]));
+            key = v != v ? (pos == K ? FBits<double>::bits(kInf) + 1ull : 0ull)
+                         : FBits<double>::bits(v) + 1ull;
+        }
+        const unsigned kh = (unsigned)(key >> 32), kl = (unsigned)key;
+        const unsigned mh = __reduce_max_sync(tm.mask, kh);
+        const unsigned ml = __reduce_max_sync(tm.mask, kh == mh ? kl : 0u);
+        const bool top = kh == mh && kl == ml;
+        const int wi = (int)__reduce_min_sync(tm.mask, top ? (unsigned)pos : 0xffffffffu);
+        const unsigned hold = __ballot_sync(tm.mask, pos == wi) & tm.mask;
+        const int pl = (__ffs(hold) - 1) & (T - 1);
+        if (lane == K) owner = pl;
+        if (lane == pl) pos = K;
+        else if (pos == K) pos = wi;
+        const unsigned b = slot(K);
+        if (lane == pl) put_row<K>(b);
+        __syncwarp(tm.mask);
+        TF p[N];
+        get_row<K>(b, p);
+        const TF akk = p[K];
+        const bool dok = akk != TF(0);
+        if (!dok && info == 0) info = K + 1;
+        const TF rk = (kRecip && dok) ? TF(1) / akk : TF(0);
+        if (dok && pos > K) {
+            const TF l = kRecip ? r[K] * rk : r[K] / akk;
+            r[K] = l;
+#pragma unroll
+            for (int j = K + 1; j < N; ++j) r[j] = A::msub(l, p[j], r[j]);
+        }
+        // the reciprocal replaces the pivot for the back substitution
+        if (dok && kRecip && lane == pl) r[K] = rk;
+    }
+    template <int K> __device__ __forceinline__ void eliminate(const Team<T>& tm) {
+        if constexpr (K < N) {
+            step<K>(tm);
+            eliminate<K + 1>(tm);
+        }
+    }
+
+    // J into the lane's row, factor_matrix's scaling, then the elimination (lu.jl:24-64).
+    template <class Fam>
+    __device__ __forceinline__ void factor(const Team<T>& tm, const Fam& fam, const typename Fam::JState& js) {
+        const int lane = tm.lane;
+        const bool mine = lane < N;
+        const int i = mine ? lane : N - 1;
+        constexpr bool same = sizeof(TF) == sizeof(double);
+        unsigned long long mb = 0ull;
+        if constexpr (same) {
+#pragma unroll
+            for (int k = 0; k < N; ++k) {
+                r[k] = fam.Jent(js, i, k);
+                const unsigned long long bk = FBits<double>::bits(r[k]) & ~FBits<double>::sign_mask;
+                mb = bk > mb ? bk : mb;
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < N; ++k) {
+                const unsigned long long bk =
+                    FBits<double>::bits(fam.Jent(js, i, k)) & ~FBits<double>::sign_mask;
+                mb = bk > mb ? bk : mb;
+            }
+        }
+        if (!mine) mb = 0ull;
+        const double mm = FBits<double>::from(tm.umax(mb));
+        if constexpr (same) {
+            int ex = 0;
+            if (isfin(mm) && mm != 0.0) {
+                ex = jexponent(mm);
+                ex = ex > 1023 ? 1023 : (ex < -1023 ? -1023 : ex);
+            }
+            e = ex < 0 ? ex : 0;
+            if (e < 0) {
+#pragma unroll
+                for (int k = 0; k < N; ++k) r[k] = scale2_in(r[k], -e);  // -e in [1, 1023]
+            }
+        } else {
+            e = (isfin(mm) && mm != 0.0) ? max(-1023, min(1023, jexponent(mm))) : 0;
+#pragma unroll
+            for (int k = 0; k < N; ++k) {
+                const double v = fam.Jent(js, i, k);
+                r[k] = TF(e == 0 ? v : scale2_in(v, -e));  // -e in [-1023, 1023]
+            }
+        }
+        if (!mine) {
+#pragma unroll
+            for (int k = 0; k < N; ++k) r[k] = TF(0);
+        }
+        info = 0;
+        pos = mine ? lane : -1;
+        owner = lane;
+        eliminate<0>(tm);
+        __syncwarp(tm.mask);  // the last buffer is read before a later factor writes it
+    }
+
+    // The substitution steps, instantiated one by one (a loop over them is not always
+    // unrolled, and a row indexed at run time would live in local memory).
+    template <int K> __device__ __forceinline__ void forward(const Team<T>& tm, TF& x) const {
+        if constexpr (K < N) {
+            const TF xk = tm.bcast(x, tm.bcast(owner, K));
+            if (pos > K) x = A::msub(r[K], xk, x);
+            forward<K + 1>(tm, x);
+        }
+    }
+    template <int K> __device__ __forceinline__ void backward(const Team<T>& tm, TF& x) const {
+        if constexpr (K >= 0) {
+            if (pos == K) x = kRecip ? x * r[K] : x / r[K];
+            const TF xk = tm.bcast(x, tm.bcast(owner, K));
+            if (pos >= 0 && pos < K) x = A::msub(r[K], xk, x);
+            backward<K - 1>(tm, x);
+        }
+    }
+    // lu.jl:67-92 on the distributed right-hand side: lane i enters with entry i and leaves
+    // with entry i of the solution. The exchanges applied to the right-hand side move entry i
+    // to position pos, where lane i already holds it; the substitutions run over positions,
+    // and the unknown of column k is found in lane owner(k).
+    __device__ __forceinline__ void backsolve(const Team<T>& tm, TF& x) const {
+        forward<0>(tm, x);
+        backward<N - 1>(tm, x);
+        x = tm.bcast(x, owner);
+    }
+
+    // ldiv!!: same type (factors.jl:931-936) or mixed type (factors.jl:943-949).
+    __device__ __forceinline__ double ldiv(const Team<T>& tm, const WarpVec<N, T, F>& wv, double rr) const {
+        const bool mine = tm.lane < N;
+        if constexpr (sizeof(TF) == sizeof(double)) {
+            // rhs_exponent (factors.jl:880-885)
+            const int m = wv.exponent(rr, mine);
+            const int lo = e < 0 ? e : 0;
+            const int aa = m > 0 ? 0 : (m < lo ? lo : m);
+            const int bb = m - (1023 - headroom(N));
+            const int k = aa > bb ? aa : bb;
+            TF x = k == 0 ? rr : scale2_in(rr, -k);  // -k in [-6, 1023]
+            backsolve(tm, x);
+            const int e2 = k - e;
+            return e2 == 0 ? double(x) : scale2_in(double(x), e2);  // e2 in [0, 1029]
+        } else {
+            const double s = wv.maxabs(rr);
+            if (s == 0.0) return 0.0;
+            TF x = TF(kRecip ? __dmul_rn(rr, __drcp_rn(s)) : __ddiv_rn(rr, s));
+            backsolve(tm, x);
+            int ex = 0;
+            double frac = isfin(s) ? frexp(s, &ex) : s;
+            if (!isfin(s)) ex = 0;
+            double d = __dmul_rn(double(x), frac);
+            const int E = ex - e;
+            return (E >= -1074 && E <= 2046) ? scale2_in(d, E) : ldexp2_slow(d, E);
+        }
+    }
+};
+
 // The pivoted LU of an N x N matrix in shared memory, rows at a + i * LD; lane k keeps the
-// pivot of column k in `piv`.
-template <int N, int T, bool F, class TF> struct WarpLU {
+// pivot of column k in `piv`. The factor of the 16-lane teams (n = 12 and 16), two systems to a
+// warp: measured faster there than the register factor below (n = 12: 1.65 against 1.96 ms for
+// 262,144 systems), whose pivot search and row broadcasts cost about what they save.
+template <int N, int T, bool F, class TF> struct WarpSmemLU {
     static constexpr int LD = warp_ld(N);
     // the fused factor divides by multiplying with pivot reciprocals (see LUFactor); in the
     // back substitution that takes a division off each of the N sequential steps
@@ -448,6 +677,15 @@ template <int N, int T, bool F, class TF> struct WarpLU {
     }
 };
 
+// The factor of a team: rows in registers for the 32-lane teams, in shared memory for 16.
+template <int N, int T, bool F, class TF>
+using WarpLU = typename std::conditional<T == 32, WarpRegLU<N, T, F, TF>, WarpSmemLU<N, T, F, TF>>::type;
+
+// Shared memory of a system's factor, in doubles.
+template <int N, int T> __host__ __device__ constexpr int warp_lu_doubles() {
+    return T == 32 ? 2 * (((N + 1) / 2) * 2) : N * warp_ld(N);
+}
+
 template <class Fam, int T, bool F, bool Mixed, bool PlainRef> struct WarpSolver {
     static constexpr int N = Fam::N, LD = warp_ld(N);
     using A = Arith<F>;
@@ -456,7 +694,7 @@ template <class Fam, int T, bool F, bool Mixed, bool PlainRef> struct WarpSolver
     const GsbMethod& m;
     const GsbOptions& o;
     const Team<T>& tm;
-    double* lu;  // N x LD doubles of shared memory for the factor (a Float32 factor uses half)
+    double* lu;  // the factor's shared memory (warp_lu_doubles<N, T>() doubles)
     WarpVec<N, T, F> wv;
 
     __device__ WarpSolver(const Fam& f, const GsbMethod& mm, const GsbOptions& oo,

@@ -166,10 +166,14 @@ typedef enum {
  *   refinement                   = NoRefinement() / Refinement(eta, maxiter)
  *   globalization                = Static(alpha) / Backtracking(c1, p, maxiter) /
  *                                  LevenbergMarquardt(mu0, mu_min, mu_max, mu_decrease,
- *                                                     mu_increase, rho_accept; scaling = :none)
- * regularization must be 0 (the default); reuse, DogLeg and the matrix-free methods are not
- * part of this ABI. `arithmetic` and `threads_per_system` have no counterpart in the reference:
- * they choose the device arithmetic (GsbArithmetic) and how many lanes solve one system.
+ *                                                     mu_increase, rho_accept; scaling = :none) /
+ *                                  DogLeg(radius)
+ *   reuse                        = Newton(reuse = k)
+ * regularization must be 0 (the default); the matrix-free methods are not part of this ABI.
+ * reuse >= 1 and DogLeg run with a Float64 LU factor, no refinement and one thread per system
+ * (n <= 8); other combinations return GSB_ERR_UNSUPPORTED. `arithmetic` and
+ * `threads_per_system` have no counterpart in the reference: they choose the device arithmetic
+ * (GsbArithmetic) and how many lanes solve one system.
  */
 typedef struct {
     int32_t linsolve;         /* GsbLinsolve */
@@ -335,14 +339,18 @@ GSB_API int gsb_solve_batch_host(const GsbProblem* prob, const GsbMethod* method
  * on the first call with a given set of arguments and replayed after. `table` (nullable) gives,
  * per bucket in the order of the sizes above, the threads per system (0: the default of the
  * size; 1 up to n = 8, or 2, 4, 8 lanes for n = 6 and 8 under fused arithmetic; 16 or 32 lanes
- * for n = 12 and 16; 32 for n = 24 and 32) and the persistent CTAs per SM (0: as many as fit).
- * The call returns after the batch is solved; a size outside the set returns GSB_ERR_ARGUMENT
- * (its systems are left untouched). All pointers are device pointers.
+ * for n = 12 and 16; 32 for n = 24 and 32), the persistent CTAs per SM (0: as many as fit) and
+ * the systems per CTA of the warp form (n >= 12: a CTA of systems_per_cta x threads_per_system
+ * lanes, a multiple of 32 and at most 128; 0: 128 lanes; the other forms take 0). The call
+ * returns after the batch is solved; a size outside the set returns GSB_ERR_ARGUMENT (its
+ * systems are left untouched). All pointers are device pointers.
  */
 #define GSB_UNEVEN_BUCKETS 9
 typedef struct {
     int32_t threads_per_system;
     int32_t ctas_per_sm;
+    int32_t systems_per_cta;
+    int32_t pad_;
 } GsbBucketConfig;
 
 GSB_API int gsb_uneven_sizes(int32_t* sizes_out /* GSB_UNEVEN_BUCKETS entries */);

@@ -91,7 +91,14 @@ def test_uneven_tables_replay_and_count_form(gsb, oracle):
     tab = [(0, 1)] * 9
     tab[5] = (32, 1)
     tab[6] = (32, 2)
-    for table in (None, tab, tab):  # the third call replays the graph of the second
+    # the warp form's CTA size chosen per bucket: 32 lanes (two 16-lane systems) at n = 12, one
+    # 32-lane system at n = 16 and 24, two at n = 32
+    tab3 = [(0, 0, 0)] * 9
+    tab3[5] = (16, 0, 2)
+    tab3[6] = (32, 0, 1)
+    tab3[7] = (32, 3, 1)
+    tab3[8] = (32, 0, 2)
+    for table in (None, tab, tab, tab3):  # the third call replays the graph of the second
         xg, sg = _run(gsb, m, opts, sizes, X0, P, table=table)
         assert xg.tobytes() == xo.tobytes()
         assert sg.tobytes() == so.tobytes()
@@ -132,9 +139,27 @@ def test_uneven_rejections(gsb):
                                gsb.Newton(arithmetic="unfused"), table=[(0, 0)] * 4 + [(2, 0)] + [(0, 0)] * 4)
 
 
+def test_uneven_cta_size_rejections(gsb):
+    import torch
+
+    sizes, X0, P = c4(64)
+    m = gsb.Newton(globalization=gsb.Backtracking())
+    args = (_dev(X0), None, torch.tensor(sizes, device="cuda"), _dev(P), m)
+    for b, cfg in ((4, (1, 0, 2)),     # the one-thread form has a fixed CTA size
+                   (8, (32, 0, 8)),    # 256 lanes: above the warp form's 128
+                   (5, (16, 0, 1))):   # 16 lanes: not a whole warp
+        tab = [(0, 0, 0)] * 9
+        tab[b] = cfg
+        with pytest.raises(gsb.ArgumentError):
+            gsb.solve_batch_uneven(*args, table=tab)
+
+
 def test_autotuner_table(gsb):
     m = gsb.Newton(globalization=gsb.Backtracking())
     table, timings = gsb.tune.autotune_uneven(m, sample=2048, reps=1, sizes=(8, 16))
-    assert len(table) == 9
+    assert len(table) == 9 and all(len(t) == 3 for t in table)
     assert table[4][0] in (1, 2, 4, 8) and table[6][0] in (16, 32)
+    assert table[4][2] == 0 and table[6][2] * table[6][0] in (32, 64, 128)
     assert set(timings) == {8, 16} and all(v > 0 for v in timings[8].values())
+    # both CTA sizes and team sizes of n = 16 were timed
+    assert {k.split("/")[2] for k in timings[16]} == {"s1", "s2", "s4", "s8"}

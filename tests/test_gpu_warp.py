@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 from test_gpu_parity import OPTS, check_parity, run_gpu
-from workloads import cubic_affine, cubic_affine_illcond, cubic_affine_pivoting
+from workloads import cubic_affine, cubic_affine_illcond, cubic_affine_pivoting, rng
 
 pytestmark = pytest.mark.gpu
 
@@ -68,3 +68,56 @@ def test_warp_soa_order(gsb, oracle):
     order = np.random.default_rng(1).permutation(X0.shape[0])
     xg, sg = run_gpu(gsb, prob, m, X0, P, opts, order=order)
     check_parity(xg, sg, xo, so, bitwise=True)
+
+
+def _hostile(n, nsys=768):
+    """Cubic-affine systems that reach every branch of the factor: integer-valued A (ties in the
+    pivot search, exact zeros), a zero row (singular at the first column), two equal rows
+    (singular at a later column), rows scaled by 2^-600 and 2^+500 (the factor's exponent
+    scaling), and starts with a NaN or an Inf entry."""
+    g = rng(60 + n)
+    A = np.round(g.normal(0.0, 1.5, (nsys, n, n)))
+    A[:, np.arange(n), np.arange(n)] += np.where(g.random((nsys, n)) < 0.5, 0.0, n / 4)
+    b = np.round(g.uniform(-2.0, 2.0, (nsys, n)))
+    X0 = np.zeros((nsys, n))
+    kind = np.arange(nsys) % 6
+    rows = g.integers(0, n, (nsys, 2))
+    for s in np.flatnonzero(kind == 1):
+        A[s, rows[s, 0], :] = 0.0
+    for s in np.flatnonzero(kind == 2):
+        if rows[s, 0] != rows[s, 1]:
+            A[s, rows[s, 1], :] = A[s, rows[s, 0], :]
+    A[kind == 3] *= 2.0 ** -600
+    b[kind == 3] *= 2.0 ** -600
+    A[kind == 4] *= 2.0 ** 500
+    X0[kind == 5, 0] = np.where(np.arange((kind == 5).sum()) % 2 == 0, np.nan, np.inf)
+    P = np.concatenate([A.transpose(0, 2, 1).reshape(nsys, n * n), b], axis=1)
+    return X0, np.ascontiguousarray(P)
+
+
+def _same_statuses(sg, so):
+    """Every status field bit for bit, except that a NaN equals any NaN: a residual norm made
+    from an Inf start (Inf - Inf) is the device's NaN, whose sign bit differs from the x86 one
+    the oracle's arithmetic makes."""
+    for name in sg.dtype.names:
+        a, b = sg[name], so[name]
+        if a.dtype.kind == "f":
+            same = (a.view(np.uint64) == b.view(np.uint64)) | (np.isnan(a) & np.isnan(b))
+            assert same.all(), f"{name} differs at {np.flatnonzero(~same)[:8]}"
+        else:
+            assert np.array_equal(a, b), f"{name} differs at {np.flatnonzero(a != b)[:8]}"
+
+
+@pytest.mark.parametrize("n", SIZES)
+def test_warp_ties_singular_and_scaling(gsb, oracle, n):
+    X0, P = _hostile(n)
+    prob = gsb.NonlinearProblem(gsb.CubicAffine(n))
+    opts = gsb.Options(**OPTS)
+    for lin in (gsb.LUFactorization(), gsb.LUFactorization("float32")):
+        m = gsb.Newton(linsolve=lin, globalization=gsb.Backtracking(), arithmetic="unfused")
+        xg, sg = run_gpu(gsb, prob, m, X0, P, opts)
+        xo, so = oracle.solve_batch(prob, m, X0.copy(), P, opts)
+        assert xg.tobytes() == xo.tobytes()
+        _same_statuses(sg, np.ascontiguousarray(so))
+        # every kind of system is present: successes, singular factors, non-finite starts
+        assert {0, 3, 4} <= set(np.unique(so["code"]).tolist())

@@ -655,9 +655,19 @@ __global__ void __launch_bounds__(kThreads, (warp_min_blocks<Fam, T>())) warp_ke
         } else if (i < r.n) {
             const int64_t idx = r.order ? r.order[i] - L.order_base : i;
             const double* pb = param_block(L, idx, NP);
-            for (int k = tid % T; k < NP; k += T)
-                sys[Fam::place(k)] = L.p_layout == GSB_SOA ? __ldg(L.P + (int64_t)k * L.nsys + idx)
-                                                           : __ldg(pb + k);
+            if (L.p_layout == GSB_SOA) {
+                for (int k = tid % T; k < NP; k += T)
+                    sys[Fam::place(k)] = __ldg(L.P + (int64_t)k * L.nsys + idx);
+            } else {
+                // the team's block by asynchronous 8-byte copies, all in flight at once (a
+                // ragged bucket or an `order` reaches here)
+                for (int k = tid % T; k < NP; k += T) {
+                    const unsigned dst = smem_addr(sys + Fam::place(k));
+                    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(dst), "l"(pb + k)
+                                 : "memory");
+                }
+                asm volatile("cp.async.wait_all;" ::: "memory");
+            }
         }
         __syncthreads();
         if (i >= r.n) return;

@@ -875,55 +875,113 @@ __device__ __forceinline__ int uneven_bucket(int n) {
 // The bucketing state of one call, in device memory (zeroed at the start of each run).
 struct UnevenWork {
     unsigned long long count[GSB_UNEVEN_BUCKETS];
-    unsigned long long cursor[GSB_UNEVEN_BUCKETS];
     unsigned long long range[GSB_UNEVEN_BUCKETS][2];  // {count, first} in the index list
     unsigned long long queue[GSB_UNEVEN_BUCKETS];
     unsigned long long bad;  // systems whose size is outside the set
     unsigned long long tally[6];
 };
 
-// Sizes to bucket counts, one atomic per bucket present in a warp.
-__global__ void uneven_count(const int32_t* n, int64_t nsys, UnevenWork* w) {
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < nsys; s += stride) {
-        const int b = uneven_bucket(n[s]);
-        const unsigned act = __activemask();
-        const unsigned grp = __match_any_sync(act, b);
-        if ((threadIdx.x & 31) == __ffs(grp) - 1) {
-            if (b < 0) atomicAdd(&w->bad, (unsigned long long)__popc(grp));
-            else atomicAdd(&w->count[b], (unsigned long long)__popc(grp));
-        }
-    }
+// The bucketing takes three passes over the sizes, each CTA over its own contiguous range of
+// systems (`chunk` each), with no global atomics: its per-bucket counts, then one CTA turns them
+// into each CTA's first index per bucket, then each CTA writes its systems' indices in order.
+// A bucket's index list is therefore in the order of the batch, so that neighbouring systems of
+// a bucket stay neighbours in memory.
+constexpr int kBucketThreads = 256;
+
+__device__ __forceinline__ int bucket_slot(int32_t n) {
+    const int b = uneven_bucket(n);
+    return b < 0 ? GSB_UNEVEN_BUCKETS : b;  // the last slot holds the sizes outside the set
 }
 
-// Bucket b's indices start after those of the smaller sizes.
-__global__ void uneven_ranges(UnevenWork* w) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    unsigned long long first = 0;
-    for (int b = 0; b < GSB_UNEVEN_BUCKETS; ++b) {
-        w->range[b][0] = w->count[b];
-        w->range[b][1] = first;
-        first += w->count[b];
-    }
-}
-
-// Each system's index into its bucket's part of the list (the order within a bucket is that of
-// the atomics; every system is solved alone, so it does not change any result).
-__global__ void uneven_scatter(const int32_t* n, int64_t nsys, UnevenWork* w, int64_t* list) {
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+// Per-CTA counts of each bucket, cta_count[c * GSB_UNEVEN_BUCKETS + b].
+__global__ void __launch_bounds__(kBucketThreads) uneven_count(const int32_t* n, int64_t nsys,
+                                                               int64_t chunk, UnevenWork* w,
+                                                               unsigned* cta_count) {
+    __shared__ unsigned cnt[GSB_UNEVEN_BUCKETS + 1];
+    if (threadIdx.x <= GSB_UNEVEN_BUCKETS) cnt[threadIdx.x] = 0u;
+    __syncthreads();
+    const int64_t lo = (int64_t)blockIdx.x * chunk;
+    const int64_t hi = lo + chunk < nsys ? lo + chunk : nsys;
     const int lane = threadIdx.x & 31;
-    for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < nsys; s += stride) {
-        const int b = uneven_bucket(n[s]);
-        const unsigned act = __activemask();
-        const unsigned grp = __match_any_sync(act, b);
-        const int leader = __ffs(grp) - 1;
-        unsigned long long at = 0;
-        if (lane == leader && b >= 0) at = atomicAdd(&w->cursor[b], (unsigned long long)__popc(grp));
-        at = __shfl_sync(grp, at, leader);
-        if (b >= 0) {
-            const unsigned below = grp & ((1u << lane) - 1u);
-            list[w->range[b][1] + at + __popc(below)] = s;
+    for (int64_t s = lo + threadIdx.x; s < hi; s += kBucketThreads) {
+        const int slot = bucket_slot(n[s]);
+        const unsigned grp = __match_any_sync(__activemask(), slot);
+        if (lane == __ffs(grp) - 1) atomicAdd(&cnt[slot], (unsigned)__popc(grp));
+    }
+    __syncthreads();
+    if (threadIdx.x < GSB_UNEVEN_BUCKETS)
+        cta_count[(int64_t)blockIdx.x * GSB_UNEVEN_BUCKETS + threadIdx.x] = cnt[threadIdx.x];
+    if (threadIdx.x == GSB_UNEVEN_BUCKETS && cnt[GSB_UNEVEN_BUCKETS])
+        atomicAdd(&w->bad, (unsigned long long)cnt[GSB_UNEVEN_BUCKETS]);
+}
+
+// One CTA of GSB_UNEVEN_BUCKETS warps: warp b scans bucket b's per-CTA counts into each CTA's
+// first index (in place), after the indices of the smaller sizes; the bucket ranges go to w.
+__global__ void uneven_ranges(UnevenWork* w, unsigned* cta_count, int ctas) {
+    __shared__ unsigned long long total[GSB_UNEVEN_BUCKETS];
+    const int b = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int per = (ctas + 31) / 32;
+    const int c0 = lane * per, c1 = c0 + per < ctas ? c0 + per : ctas;
+    unsigned long long sum = 0;
+    for (int c = c0; c < c1; ++c) sum += cta_count[(int64_t)c * GSB_UNEVEN_BUCKETS + b];
+    unsigned long long incl = sum;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const unsigned long long o = __shfl_up_sync(0xffffffffu, incl, off);
+        if (lane >= off) incl += o;
+    }
+    if (lane == 31) total[b] = incl;
+    __syncthreads();
+    unsigned long long first = 0;
+    for (int q = 0; q < b; ++q) first += total[q];
+    unsigned long long at = first + incl - sum;
+    for (int c = c0; c < c1; ++c) {
+        unsigned* slot = &cta_count[(int64_t)c * GSB_UNEVEN_BUCKETS + b];
+        const unsigned k = *slot;
+        *slot = (unsigned)at;
+        at += k;
+    }
+    if (lane == 0) {
+        w->count[b] = total[b];
+        w->range[b][0] = total[b];
+        w->range[b][1] = first;
+    }
+}
+
+// Each system's index into its bucket's part of the list, tile by tile in the batch's order.
+__global__ void __launch_bounds__(kBucketThreads) uneven_scatter(const int32_t* n, int64_t nsys,
+                                                                 int64_t chunk,
+                                                                 const unsigned* cta_first,
+                                                                 int64_t* list) {
+    constexpr int W = kBucketThreads / 32, B = GSB_UNEVEN_BUCKETS;
+    __shared__ unsigned base[B], tile_total[B];
+    __shared__ unsigned warp_first[W][B + 1];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    if (tid < B) base[tid] = cta_first[(int64_t)blockIdx.x * B + tid];
+    const int64_t lo = (int64_t)blockIdx.x * chunk;
+    const int64_t hi = lo + chunk < nsys ? lo + chunk : nsys;
+    for (int64_t tile = lo; tile < hi; tile += kBucketThreads) {  // the same count in every thread
+        if (tid < W * (B + 1)) warp_first[tid / (B + 1)][tid % (B + 1)] = 0u;
+        __syncthreads();
+        const int64_t s = tile + tid;
+        const int slot = s < hi ? bucket_slot(n[s]) : B;
+        const unsigned grp = __match_any_sync(0xffffffffu, slot);
+        const unsigned rank = __popc(grp & ((1u << lane) - 1u));
+        if (lane == __ffs(grp) - 1) warp_first[warp][slot] = (unsigned)__popc(grp);
+        __syncthreads();
+        if (tid < B) {
+            unsigned run = 0;
+            for (int q = 0; q < W; ++q) {
+                const unsigned k = warp_first[q][tid];
+                warp_first[q][tid] = run;
+                run += k;
+            }
+            tile_total[tid] = run;
         }
+        __syncthreads();
+        if (slot < B) list[(int64_t)base[slot] + warp_first[warp][slot] + rank] = s;
+        __syncthreads();
+        if (tid < B) base[tid] += tile_total[tid];
     }
 }
 
@@ -952,6 +1010,7 @@ struct UnevenPlan {
     bool ready = false;
     UnevenKey key{};
     gsb::UnevenWork* work = nullptr;
+    unsigned* cta_count = nullptr;  // the bucketing's per-CTA counts (kBucketCtasPerSm x SMs x 9)
     int64_t* list = nullptr;
     int64_t list_cap = 0;
     cudaStream_t cs = nullptr;
@@ -962,6 +1021,7 @@ struct UnevenPlan {
 };
 std::mutex g_uneven_mu;
 UnevenPlan g_uneven[64];
+constexpr int kBucketCtasPerSm = 8;  // CTAs of the bucketing kernels
 
 int uneven_streams(UnevenPlan& p) {
     if (p.cs) return 0;
@@ -1040,15 +1100,20 @@ int uneven_capture(UnevenPlan& p, const UnevenKey& k, bool want_tally) {
         cudaGraphExecDestroy(p.exec);
         p.exec = nullptr;
     }
-    const unsigned cgrid = (unsigned)std::min<int64_t>((k.nsys + 255) / 256, (int64_t)sms * 8);
+    // the bucketing's CTAs, each over a contiguous range of `chunk` systems
+    const unsigned cgrid = (unsigned)std::min<int64_t>(
+        (k.nsys + gsb::kBucketThreads - 1) / gsb::kBucketThreads, (int64_t)sms * kBucketCtasPerSm);
+    const int64_t chunk = (k.nsys + cgrid - 1) / cgrid;
     unsigned* fault = fault_word();  // allocated (once) before the capture begins
     cudaGraph_t g = nullptr;
     if (int rc = cuda_err(cudaStreamBeginCapture(p.cs, cudaStreamCaptureModeThreadLocal), "capture"))
         return rc;
     cudaMemsetAsync(p.work, 0, sizeof(gsb::UnevenWork), p.cs);
-    gsb::uneven_count<<<cgrid, 256, 0, p.cs>>>(k.n, k.nsys, p.work);
-    gsb::uneven_ranges<<<1, 32, 0, p.cs>>>(p.work);
-    gsb::uneven_scatter<<<cgrid, 256, 0, p.cs>>>(k.n, k.nsys, p.work, p.list);
+    gsb::uneven_count<<<cgrid, gsb::kBucketThreads, 0, p.cs>>>(k.n, k.nsys, chunk, p.work,
+                                                              p.cta_count);
+    gsb::uneven_ranges<<<1, 32 * GSB_UNEVEN_BUCKETS, 0, p.cs>>>(p.work, p.cta_count, (int)cgrid);
+    gsb::uneven_scatter<<<cgrid, gsb::kBucketThreads, 0, p.cs>>>(k.n, k.nsys, chunk, p.cta_count,
+                                                                p.list);
     cudaEventRecord(p.fork, p.cs);
     // the heaviest buckets (largest n) start first, so that the light ones fill the tail
     for (int b = GSB_UNEVEN_BUCKETS - 1; b >= 0; --b) {
@@ -1094,6 +1159,8 @@ int gsb_solve_batch_uneven(const GsbMethod* method, const GsbOptions* opt, doubl
     if (s_kind != GSB_STATUS64 && s_kind != GSB_CODES) return set_err(GSB_ERR_ARGUMENT, "s_kind");
     if (tally) std::memset(tally, 0, sizeof(*tally));
     if (nsys == 0) return 0;
+    if (nsys >= (int64_t)1 << 32)
+        return set_err(GSB_ERR_DIMENSION, "a ragged batch takes fewer than 2^32 systems");
     if (!X || !S || !P || !n || !x_off || !p_off)
         return set_err(GSB_ERR_ARGUMENT, "null X, S, P, n, x_off or p_off");
     UnevenKey key{};
@@ -1116,6 +1183,14 @@ int gsb_solve_batch_uneven(const GsbMethod* method, const GsbOptions* opt, doubl
     if (int rc = uneven_streams(p)) return rc;
     if (!p.work) {
         if (int rc = cuda_err(cudaMalloc(&p.work, sizeof(gsb::UnevenWork)), "cudaMalloc")) return rc;
+    }
+    if (!p.cta_count) {
+        int sms = 0;
+        if (int rc = cuda_err(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev),
+                              "attr"))
+            return rc;
+        const size_t bytes = (size_t)sms * kBucketCtasPerSm * GSB_UNEVEN_BUCKETS * sizeof(unsigned);
+        if (int rc = cuda_err(cudaMalloc(&p.cta_count, bytes), "cudaMalloc")) return rc;
     }
     if (p.list_cap < nsys) {
         if (p.list) cudaFree(p.list);

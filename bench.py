@@ -384,7 +384,11 @@ def main():
     xo, so = O.solve_batch(prob, plain, X0_h.copy(), P_h, opts, nthreads=nt)
     solved = {}
     fp64_err = {}
-    for name, m in (("plain_fp64", plain), ("fp32_lu_refinement", mixed)):
+    # the mixed form with its line-search trials in Float32 too (a labelled departure)
+    trial32 = G.Newton(linsolve=G.LUFactorization("float32"), refinement=G.Refinement(),
+                       globalization=G.Backtracking(), trial="float32")
+    for name, m in (("plain_fp64", plain), ("fp32_lu_refinement", mixed),
+                    ("fp32_lu_refinement_fp32_trials", trial32)):
         X.copy_(X0)
         G.solve_batch(X, S, prob, m, ps, options=opts)
         st = G.statuses(S)
@@ -445,6 +449,7 @@ def main():
     with Clocks(local) as clk:
         ms_plain = timed(plain, args.steps, args.warmup)
         ms_mixed = timed(mixed, args.steps, args.warmup)
+        ms_trial32 = timed(trial32, args.steps, args.warmup)
     clocks = clk.summary()
     chosen_name = "fp32_lu_refinement" if solved["fp32_lu_refinement"] / ms_mixed >= \
         solved["plain_fp64"] / ms_plain else "plain_fp64"
@@ -551,6 +556,13 @@ def main():
             "fp32_lu_refinement": {"systems_per_s": sum_over_ranks(solved["fp32_lu_refinement"]) / (ms_mixed * 1e-3),
                                    "ms_per_step": ms_mixed, "solved": solved["fp32_lu_refinement"],
                                    "fp64_oracle_max_rel_err": fp64_err["fp32_lu_refinement"]},
+            "fp32_lu_refinement_fp32_trials": {
+                "systems_per_s": sum_over_ranks(solved["fp32_lu_refinement_fp32_trials"]) /
+                                 (ms_trial32 * 1e-3),
+                "ms_per_step": ms_trial32, "solved": solved["fp32_lu_refinement_fp32_trials"],
+                "fp64_oracle_max_rel_err": fp64_err["fp32_lu_refinement_fp32_trials"],
+                "departure": "trial increments alpha d in Float32, measured slope from the held "
+                             "residual (Float32 fold); residuals, norms and tests Float64"},
             "chosen_over_plain": value / plain_value,
         },
         "e2e": {"value": e2e_value, "unit": "systems/s", "h2d_bytes_per_step": h2d,

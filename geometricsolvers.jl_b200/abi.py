@@ -131,7 +131,7 @@ class GsbMethod(ctypes.Structure):
         ("arithmetic", ctypes.c_int32),
         ("threads_per_system", ctypes.c_int32),
         ("reuse", ctypes.c_int32),
-        ("pad_", ctypes.c_int32),
+        ("trial_precision", ctypes.c_int32),
         ("dogleg_radius", ctypes.c_double),
     ]
 

@@ -235,10 +235,24 @@ class Newton:
     # Lanes of a warp that share one system on the device (1, 2, 4, 8, 16, 32), or None for the
     # library's tuned choice; no reference field.
     threads_per_system: Optional[int] = None
+    # The precision of the line-search trials: None (Float64, the reference's) or "float32" (a
+    # departure with no reference field: each trial's increment alpha d in Float32 and the
+    # measured slope from the held residual; residuals, norms and tests stay Float64). Takes a
+    # Float32 LUFactorization, no reuse, Backtracking or Static.
+    trial: Optional[str] = None
 
     def __post_init__(self):
         if self.arithmetic not in ("fused", "unfused"):
             raise ArgumentError("arithmetic must be 'fused' or 'unfused'")
+        if self.trial not in (None, "float64", "float32"):
+            raise ArgumentError("trial must be None, 'float64' or 'float32'")
+        if self.trial == "float32":
+            if not (isinstance(self.linsolve, LUFactorization)
+                    and _precision(self.linsolve.TF) == abi.GSB_F32):
+                raise ArgumentError("Float32 line-search trials go with LUFactorization('float32')")
+            if self.reuse is not None or not isinstance(self.globalization, (Backtracking, Static)):
+                raise ArgumentError("Float32 line-search trials take no reuse and Backtracking "
+                                    "or Static")
         if self.threads_per_system not in (None, 1, 2, 4, 8, 16, 32):
             raise ArgumentError("threads_per_system must be None or one of 1, 2, 4, 8, 16, 32")
         if isinstance(self.refinement, bool):
@@ -297,6 +311,7 @@ class Newton:
             raise ArgumentError("the batch path takes regularization = 0")
         m.reuse = 0 if self.reuse is None else int(self.reuse)
         m.dogleg_radius = (g.radius or 0.0) if isinstance(g, DogLeg) else 0.0
+        m.trial_precision = abi.GSB_F32 if self.trial == "float32" else abi.GSB_F64
         m.regularization = 0.0
         m.arithmetic = abi.GSB_FUSED if self.arithmetic == "fused" else abi.GSB_UNFUSED
         m.threads_per_system = 0 if self.threads_per_system is None else self.threads_per_system

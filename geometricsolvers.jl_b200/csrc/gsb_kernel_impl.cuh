@@ -733,6 +733,16 @@ template <class Fam, bool F, int Kind> KernelEntry* kind_entry() {
     return &e;
 }
 
+// The mixed LU step (Float32 factor, refinement as the method says) with its line-search trials
+// in Float32 (kStepTrial32).
+template <class Fam, bool F> KernelEntry* trial32_entry() {
+    static KernelEntry e{newton_kernel<Fam, F, true, false, false, false, kStepTrial32>,
+                         newton_kernel<Fam, F, true, false, true, false, kStepTrial32>,
+                         ((SharedLen<Fam>::value + 1) / 2) * 2 + kThreads * newton_row_stride<Fam>(),
+                         kThreads, {}, PairsOf<Fam>::value};
+    return &e;
+}
+
 // The plain step with the static QR factor (QRFactorization, Float64, no refinement).
 template <class Fam, bool F> KernelEntry* qr_entry() {
     static KernelEntry e{newton_kernel<Fam, F, false, false, false, true>,
@@ -795,6 +805,11 @@ template <class Fam> KernelEntry* pick(bool fused, bool mixed, bool refine) {
         return fused ? qr_entry<__VA_ARGS__, true>() : qr_entry<__VA_ARGS__, false>();        \
     }
 #define GSB_DECLARE_TEAM(NAME) KernelEntry* team_##NAME(int T, bool mixed)
+#define GSB_DECLARE_TRIAL32(NAME) KernelEntry* trial32_##NAME(bool fused)
+#define GSB_DEFINE_TRIAL32(NAME, ...)                                                         \
+    KernelEntry* trial32_##NAME(bool fused) {                                                 \
+        return fused ? trial32_entry<__VA_ARGS__, true>() : trial32_entry<__VA_ARGS__, false>(); \
+    }
 #define GSB_DECLARE_KIND(NAME) KernelEntry* kind_##NAME(bool fused, int kind)
 #define GSB_DEFINE_KIND(NAME, ...)                                                            \
     KernelEntry* kind_##NAME(bool fused, int kind) {                                          \

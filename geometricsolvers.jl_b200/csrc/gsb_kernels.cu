@@ -244,6 +244,11 @@ GSB_DECLARE_KIND(cubic6);
 GSB_DECLARE_KIND(cubic8);
 GSB_DECLARE_KIND(hetero6);
 GSB_DECLARE_KIND(coupled2);
+GSB_DECLARE_TRIAL32(cubic2);
+GSB_DECLARE_TRIAL32(cubic3);
+GSB_DECLARE_TRIAL32(cubic4);
+GSB_DECLARE_TRIAL32(cubic6);
+GSB_DECLARE_TRIAL32(cubic8);
 KernelEntry* lm_expsum3_64(bool fused, bool mixed);
 KernelEntry* warp_cubic12(bool fused, bool mixed, bool refine, int T);
 KernelEntry* warp_cubic16(bool fused, bool mixed, bool refine, int T);
@@ -300,6 +305,20 @@ KernelEntry* select_kind_kernel(const GsbProblem* prob, bool fused, int kind, in
         }
     case GSB_FAMILY_HETERO6: return kind_hetero6(fused, kind);
     case GSB_FAMILY_COUPLED2: return kind_coupled2(fused, kind);
+    default: return nullptr;
+    }
+}
+
+// The kernel of the mixed step whose line-search trials run in Float32: one thread per system,
+// the cubic-affine family, a per-system parameter block.
+KernelEntry* select_trial32_kernel(const GsbProblem* prob, bool fused, int T) {
+    if (T > 1 || shared_matrix(prob) || prob->family != GSB_FAMILY_CUBIC_AFFINE) return nullptr;
+    switch (prob->n) {
+    case 2: return trial32_cubic2(fused);
+    case 3: return trial32_cubic3(fused);
+    case 4: return trial32_cubic4(fused);
+    case 6: return trial32_cubic6(fused);
+    case 8: return trial32_cubic8(fused);
     default: return nullptr;
     }
 }
@@ -419,6 +438,14 @@ int check_method(const GsbMethod* m) {
         if (!(t == 0 || t == 1 || t == 2 || t == 4 || t == 8 || t == 16 || t == 32))
             return set_err(GSB_ERR_ARGUMENT, "threads_per_system must be 0, 1, 2, 4, 8, 16 or 32");
     }
+    if (m->trial_precision != GSB_F64 && m->trial_precision != GSB_F32)
+        return set_err(GSB_ERR_ARGUMENT, "trial precision must be F64 or F32");
+    if (m->trial_precision == GSB_F32 &&
+        !(m->linsolve == GSB_LU && m->factor_precision == GSB_F32 && m->reuse == 0 &&
+          (m->globalization == GSB_BACKTRACKING || m->globalization == GSB_STATIC)))
+        return set_err(GSB_ERR_UNSUPPORTED,
+                       "Float32 line-search trials go with a Float32 LUFactorization, no reuse, "
+                       "and Backtracking or Static");
     return 0;
 }
 
@@ -470,7 +497,10 @@ int select_entry(const GsbProblem* prob, const GsbMethod* method, KernelEntry** 
         if (lm)
             return set_err(GSB_ERR_UNSUPPORTED,
                            "LevenbergMarquardt batch kernel only for least-squares families");
-        if (method->reuse > 0 || method->globalization == GSB_DOGLEG) {
+        if (method->trial_precision == GSB_F32) {
+            // the mixed step with Float32 line-search trials (checked by check_method)
+            ke = select_trial32_kernel(prob, fused, method->threads_per_system);
+        } else if (method->reuse > 0 || method->globalization == GSB_DOGLEG) {
             // factor reuse and DogLeg: the Float64 LU step without refinement
             if (method->linsolve != GSB_LU || mixed || method->refinement == GSB_REFINEMENT)
                 return set_err(GSB_ERR_UNSUPPORTED,
@@ -1156,6 +1186,8 @@ int gsb_solve_batch_uneven(const GsbMethod* method, const GsbOptions* opt, doubl
         return set_err(GSB_ERR_UNSUPPORTED, "ragged batches run Newton with LUFactorization");
     if (method->reuse > 0 || method->globalization == GSB_DOGLEG)
         return set_err(GSB_ERR_UNSUPPORTED, "ragged batches take no factor reuse and no DogLeg");
+    if (method->trial_precision == GSB_F32)
+        return set_err(GSB_ERR_UNSUPPORTED, "ragged batches take Float64 line-search trials");
     if (s_kind != GSB_STATUS64 && s_kind != GSB_CODES) return set_err(GSB_ERR_ARGUMENT, "s_kind");
     if (tally) std::memset(tally, 0, sizeof(*tally));
     if (nsys == 0) return 0;

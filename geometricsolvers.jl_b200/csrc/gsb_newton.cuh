@@ -45,7 +45,9 @@ struct DevState {
 
 // The step of the Newton solve: the method's own (plain, or the mixed-precision step), the step
 // with factor reuse, or the DogLeg trust-region step.
-enum StepKind : int { kStepNewton = 0, kStepReuse = 1, kStepDogLeg = 2 };
+// kStepTrial32: the mixed step (Float32 factor with refinement) whose line-search trials run in
+// Float32, a departure from the reference that has no counterpart there (see Solver::trial).
+enum StepKind : int { kStepNewton = 0, kStepReuse = 1, kStepDogLeg = 2, kStepTrial32 = 3 };
 
 // What a step that took the common course (Backtracking's first trial accepted at alpha = 1)
 // already formed for the stopping tests that follow it, with their own operands and operations:
@@ -774,13 +776,36 @@ struct Solver {
         return isnan(st.fnorm) ? rnorm<F, M>(Fx) : st.fnorm;
     }
 
-    // The merit of the trial x + a d: the trial iterate, its residual and norm2.
+    // The merit of the trial x + a d: the trial iterate, its residual and norm2. The Float32
+    // trial form (kStepTrial32) forms the increment a d in Float32 and adds it to the Float64
+    // iterate; the residual, its norm and every test on them stay Float64.
     __device__ __forceinline__ double trial(const double (&x)[N], const double (&d)[N], double a,
                                             double (&xt)[N], double (&Ft)[M]) const {
+        if constexpr (Kind == kStepTrial32) {
+            const float af = __double2float_rn(a);
 #pragma unroll
-        for (int i = 0; i < N; ++i) xt[i] = A::madd(a, d[i], x[i]);
+            for (int i = 0; i < N; ++i)
+                xt[i] = __dadd_rn(x[i], (double)__fmul_rn(af, __double2float_rn(d[i])));
+        } else {
+#pragma unroll
+            for (int i = 0; i < N; ++i) xt[i] = A::madd(a, d[i], x[i]);
+        }
         fam.F(xt, Ft);
         return norm2<F, M>(Ft);
+    }
+
+    // The Float32 trial form's measured slope: 2 <F(x), J(x) d> from the residual the step
+    // already holds (the reference evaluates F again at x + 0 d, the same point for a finite
+    // d) and the JVP, folded in Float32.
+    __device__ __forceinline__ double slope0_held(const double (&x)[N], const double (&Fx)[M],
+                                                  const double (&d)[N]) const {
+        double Jv[M];
+        fam.jvp(x, d, Jv);
+        float s = __fmul_rn(__double2float_rn(Fx[0]), __double2float_rn(Jv[0]));
+#pragma unroll
+        for (int i = 1; i < M; ++i)
+            s = __fmaf_rn(__double2float_rn(Fx[i]), __double2float_rn(Jv[i]), s);
+        return 2.0 * (double)s;
     }
 
     // φ′(0) = 2 <F(x), J(x) d> (src/globalization/linefunction.jl:47-52).
@@ -871,7 +896,9 @@ struct Solver {
         }
         // linesearch entry: trial step 1, the anchor slope, τ and the step floor
         double alpha = 1.0;
-        double d0 = exact ? -2.0 * phi0 : slope0(x, d);
+        double d0;
+        if constexpr (Kind == kStepTrial32) d0 = exact ? -2.0 * phi0 : slope0_held(x, Fx, d);
+        else d0 = exact ? -2.0 * phi0 : slope0(x, d);
         int code;
         double aa = alpha, pa = kNaN;
         double xt[N], Ft[M];

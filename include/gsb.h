@@ -198,7 +198,14 @@ typedef struct {
                                    0 = the library's tuned choice for the family and size */
     int32_t reuse;              /* Newton(reuse = k): k >= 1; 0 = nothing (a fresh factor at
                                    every step) */
-    int32_t pad_;
+    int32_t trial_precision;    /* GsbPrecision of the line-search trials; no counterpart in the
+                                   reference, whose trials are Float64 (GSB_F64, 0). GSB_F32 (with
+                                   a Float32 LUFactorization, no reuse, Backtracking or Static,
+                                   one thread per system, cubic-affine n in {2, 3, 4, 6, 8}) forms
+                                   each trial's increment alpha d in Float32, added to the
+                                   Float64 iterate, and takes the measured slope from the
+                                   residual the step holds with a Float32 fold; the residual,
+                                   its norm and every convergence test stay Float64. */
     double dogleg_radius;       /* DogLeg(radius): the initial trust radius, > 0; 0 = nothing
                                    (the first step sets it) */
 } GsbMethod;

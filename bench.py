@@ -1078,8 +1078,22 @@ def run_workload(args):
             forms["plain_fp64_per_bucket_launches"] = {
                 "systems_per_s": float(np.sum(okb)) / (ms_b * 1e-3), "ms_per_step": ms_b,
                 "solved": int(np.sum(okb)), "fp64_oracle_max_rel_err": float(errb.max()),
-                "launches": len(buckets)}
+                "launches": len(buckets),
+                "layout": "each bucket laid out as a uniform batch beforehand (not timed)"}
             del buckets
+            # what laying a mixed batch out by size costs a caller at the least: one read and
+            # one write of its parameter blocks and start iterates (a plain device copy)
+            P2, X2 = torch.empty_like(P), torch.empty_like(X0)
+
+            def layout_copy():
+                P2.copy_(P)
+                X2.copy_(X0)
+
+            ms_lay = _events_ms(layout_copy, args.steps, args.warmup, stream)
+            del P2, X2
+            forms["plain_fp64_per_bucket_launches"]["layout_copy_ms"] = ms_lay
+            forms["plain_fp64_per_bucket_launches"]["systems_per_s_with_layout_copy"] = \
+                float(np.sum(okb)) / ((ms_b + ms_lay) * 1e-3)
         clocks = clk.summary()
         chosen = max(("plain_fp64", "fp32_lu_refinement"), key=lambda k: forms[k]["systems_per_s"])
         value = forms[chosen]["systems_per_s"]

@@ -127,15 +127,21 @@ __device__ __forceinline__ void for_each_chunk(const Launch& L, int64_t systems_
         body((int64_t)blockIdx.x * systems_per_chunk, r);
         return;
     }
-    __shared__ unsigned long long next;
+    // Each chunk's ticket is taken one chunk ahead, so that its atomic's round trip overlaps
+    // the solve of the chunk before it: thread 0 writes slot b ^ 1 while the CTA reads slot b,
+    // and the barrier at the end of each chunk orders the two (a CTA that leaves has taken one
+    // ticket past the end, which only counts the queue further past it).
+    __shared__ unsigned long long next[2];
+    if (threadIdx.x == 0) next[0] = atomicAdd(L.queue, 1ull);
+    __syncthreads();
+    int b = 0;
     while (true) {
-        if (threadIdx.x == 0) next = atomicAdd(L.queue, 1ull);
-        __syncthreads();
-        const int64_t base = (int64_t)next * systems_per_chunk;
-        __syncthreads();  // every thread holds `next` before thread 0 takes the following chunk
+        const int64_t base = (int64_t)next[b] * systems_per_chunk;
         if (base >= r.n) return;
+        if (threadIdx.x == 0) next[b ^ 1] = atomicAdd(L.queue, 1ull);
         body(base, r);
-        __syncthreads();  // the chunk's shared memory is free again
+        __syncthreads();  // the chunk's shared memory is free again; next[b ^ 1] is written
+        b ^= 1;
     }
 }
 
@@ -383,11 +389,16 @@ __global__ void __launch_bounds__(kThreads, (min_blocks<Fam, Mixed>())) newton_k
         uint32_t phase = 0;
         SummaryPart part;  // the lane's statuses, for a fused batch summary
         int64_t c = (int64_t)blockIdx.x * W + warp;
+        // persistent launches: lane 0 takes each ticket one chunk ahead, so that the atomic's
+        // round trip overlaps the chunk before it
+        unsigned long long ahead = 0;
+        if constexpr (Persistent) {
+            if (lane == 0) ahead = atomicAdd(L.queue, 1ull);
+        }
         while (true) {
             if constexpr (Persistent) {
-                unsigned long long t = 0;
-                if (lane == 0) t = atomicAdd(L.queue, 1ull);
-                c = (int64_t)__shfl_sync(0xffffffffu, t, 0);
+                c = (int64_t)__shfl_sync(0xffffffffu, ahead, 0);
+                if (lane == 0 && c * 32 < r.n) ahead = atomicAdd(L.queue, 1ull);
             }
             if (c * 32 >= r.n) break;
             const int64_t i = c * 32 + lane;

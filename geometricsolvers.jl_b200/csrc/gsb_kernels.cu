@@ -1048,6 +1048,18 @@ struct UnevenPlan {
     cudaEvent_t fork = nullptr;
     cudaEvent_t join[GSB_UNEVEN_BUCKETS] = {};
     cudaGraphExec_t exec = nullptr;
+    // Buckets launched as one ordinary grid sized from their count (ctas_per_sm = -1): the
+    // graph copies the bucket ranges to pinned host memory and records `counted`; the host then
+    // launches those buckets on `ord`, which the caller's stream joins through `ord_done`.
+    unsigned long long* h_range = nullptr;  // {count, first} per bucket (pinned)
+    cudaStream_t ord = nullptr;
+    cudaEvent_t counted = nullptr, ord_done = nullptr;
+    bool ordinary[GSB_UNEVEN_BUCKETS] = {};
+    bool any_ordinary = false;
+    KernelEntry* ke[GSB_UNEVEN_BUCKETS] = {};
+    unsigned threads[GSB_UNEVEN_BUCKETS] = {};
+    size_t smem[GSB_UNEVEN_BUCKETS] = {};
+    int occ[GSB_UNEVEN_BUCKETS] = {};
 };
 std::mutex g_uneven_mu;
 UnevenPlan g_uneven[64];
@@ -1063,12 +1075,24 @@ int uneven_streams(UnevenPlan& p) {
         if (int rc = cuda_err(cudaEventCreateWithFlags(&p.join[b], cudaEventDisableTiming), "event"))
             return rc;
     }
+    if (int rc = cuda_err(cudaStreamCreateWithFlags(&p.ord, cudaStreamNonBlocking), "stream")) return rc;
+    if (int rc = cuda_err(cudaEventCreateWithFlags(&p.counted, cudaEventDisableTiming), "event"))
+        return rc;
+    if (int rc = cuda_err(cudaEventCreateWithFlags(&p.ord_done, cudaEventDisableTiming), "event"))
+        return rc;
+    if (int rc = cuda_err(cudaHostAlloc(reinterpret_cast<void**>(&p.h_range),
+                                        2 * GSB_UNEVEN_BUCKETS * sizeof(unsigned long long),
+                                        cudaHostAllocDefault),
+                          "cudaHostAlloc"))
+        return rc;
     return 0;
 }
 
 // The kernel of bucket b, its persistent grid and its CTA (threads, bytes of shared memory).
+// (ctas_per_sm = -1: one ordinary grid, launched by the host once the bucket's count is known;
+// `grid` is then 0 and `occ` the resident CTAs per SM of that kernel.)
 int uneven_entry(const UnevenKey& k, int b, int sms, KernelEntry** ke, unsigned* grid,
-                 unsigned* threads, size_t* smem) {
+                 unsigned* threads, size_t* smem, int* occ_out) {
     GsbProblem prob{};
     prob.family = GSB_FAMILY_CUBIC_AFFINE;
     prob.n = prob.m = kUnevenSizes[b];
@@ -1095,24 +1119,29 @@ int uneven_entry(const UnevenKey& k, int b, int sms, KernelEntry** ke, unsigned*
         *threads = (unsigned)(spc * lanes);
         *smem = (size_t)spc * (*ke)->sys_doubles * sizeof(double);
     }
-    if (!(*ke)->fn_persistent) return set_err(GSB_ERR_UNSUPPORTED, "no persistent bucket kernel");
-    // the persistent form of the bucket's kernel (set once per capture, which is rare); the
-    // attribute is the largest CTA the kernel takes, so that every CTA size fits under it
+    const int want = k.table[b].ctas_per_sm;
+    if (want < -1)
+        return set_err(GSB_ERR_ARGUMENT, "ctas_per_sm of bucket n = " +
+                                             std::to_string(kUnevenSizes[b]) +
+                                             ": -1 (an ordinary launch), 0 (as many as fit) or more");
+    const KernelFn fn = want == -1 ? (*ke)->fn : (*ke)->fn_persistent;
+    if (!fn) return set_err(GSB_ERR_UNSUPPORTED, "no persistent bucket kernel");
+    // the bucket's kernel (its attribute set once per capture, which is rare); the attribute is
+    // the largest CTA the kernel takes, so that every CTA size fits under it
     const size_t smem_max = (size_t)(*ke)->smem_doubles * sizeof(double);
-    if (int rc = cuda_err(cudaFuncSetAttribute(reinterpret_cast<const void*>((*ke)->fn_persistent),
+    if (int rc = cuda_err(cudaFuncSetAttribute(reinterpret_cast<const void*>(fn),
                                                cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                (int)std::max(smem_max, *smem)),
                           "cudaFuncSetAttribute"))
         return rc;
     int occ = 0;
     if (int rc = cuda_err(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                              &occ, reinterpret_cast<const void*>((*ke)->fn_persistent),
-                              (int)*threads, *smem),
+                              &occ, reinterpret_cast<const void*>(fn), (int)*threads, *smem),
                           "occupancy"))
         return rc;
     if (occ < 1) return set_err(GSB_ERR_UNSUPPORTED, "a bucket kernel does not fit on an SM");
-    const int want = k.table[b].ctas_per_sm;
-    *grid = (unsigned)((want > 0 && want < occ ? want : occ) * sms);
+    *occ_out = occ;
+    *grid = want == -1 ? 0u : (unsigned)((want > 0 && want < occ ? want : occ) * sms);
     return 0;
 }
 
@@ -1121,11 +1150,17 @@ int uneven_capture(UnevenPlan& p, const UnevenKey& k, bool want_tally) {
     if (int rc = cuda_err(cudaGetDevice(&dev), "cudaGetDevice")) return rc;
     if (int rc = cuda_err(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "attr"))
         return rc;
-    KernelEntry* ke[GSB_UNEVEN_BUCKETS];
-    unsigned grid[GSB_UNEVEN_BUCKETS], threads[GSB_UNEVEN_BUCKETS];
-    size_t smem[GSB_UNEVEN_BUCKETS];
-    for (int b = 0; b < GSB_UNEVEN_BUCKETS; ++b)
-        if (int rc = uneven_entry(k, b, sms, &ke[b], &grid[b], &threads[b], &smem[b])) return rc;
+    KernelEntry** ke = p.ke;
+    unsigned grid[GSB_UNEVEN_BUCKETS];
+    unsigned* threads = p.threads;
+    size_t* smem = p.smem;
+    p.any_ordinary = false;
+    for (int b = 0; b < GSB_UNEVEN_BUCKETS; ++b) {
+        if (int rc = uneven_entry(k, b, sms, &ke[b], &grid[b], &threads[b], &smem[b], &p.occ[b]))
+            return rc;
+        p.ordinary[b] = grid[b] == 0;
+        p.any_ordinary = p.any_ordinary || p.ordinary[b];
+    }
     if (p.exec) {
         cudaGraphExecDestroy(p.exec);
         p.exec = nullptr;
@@ -1144,9 +1179,18 @@ int uneven_capture(UnevenPlan& p, const UnevenKey& k, bool want_tally) {
     gsb::uneven_ranges<<<1, 32 * GSB_UNEVEN_BUCKETS, 0, p.cs>>>(p.work, p.cta_count, (int)cgrid);
     gsb::uneven_scatter<<<cgrid, gsb::kBucketThreads, 0, p.cs>>>(k.n, k.nsys, chunk, p.cta_count,
                                                                 p.list);
+    if (p.any_ordinary) {
+        // the bucket ranges for the host, which sizes the ordinary launches from them
+        cudaMemcpyAsync(p.h_range, &p.work->range[0][0],
+                        2 * GSB_UNEVEN_BUCKETS * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                        p.cs);
+        // an event node of the graph (an external record), so that the host can wait on it
+        cudaEventRecordWithFlags(p.counted, p.cs, cudaEventRecordExternal);
+    }
     cudaEventRecord(p.fork, p.cs);
     // the heaviest buckets (largest n) start first, so that the light ones fill the tail
     for (int b = GSB_UNEVEN_BUCKETS - 1; b >= 0; --b) {
+        if (p.ordinary[b]) continue;
         cudaStreamWaitEvent(p.side[b], p.fork, 0);
         Launch L{k.X, GSB_AOS, k.S, k.s_kind, k.P, GSB_AOS, p.list, 0, k.nsys, nullptr,
                  want_tally ? p.work->tally : nullptr, k.x_off, k.p_off, &p.work->queue[b],
@@ -1240,6 +1284,41 @@ int gsb_solve_batch_uneven(const GsbMethod* method, const GsbOptions* opt, doubl
     }
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
     if (int rc = cuda_err(cudaGraphLaunch(p.exec, st), "graph launch")) return rc;
+    if (p.any_ordinary) {
+        // the buckets of ordinary launches: one grid each, sized from the count the graph
+        // copied out, on their own stream beside the graph's persistent buckets
+        if (int rc = cuda_err(cudaEventSynchronize(p.counted), "bucket counts")) return rc;
+        if (int rc = cuda_err(cudaStreamWaitEvent(p.ord, p.counted, 0), "stream wait")) return rc;
+        int sms = 0;
+        if (int rc = cuda_err(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev),
+                              "attr"))
+            return rc;
+        // the ranges tile the index list in bucket order (checked before any launch reads it)
+        unsigned long long at = 0;
+        for (int b = 0; b < GSB_UNEVEN_BUCKETS; ++b) {
+            if (p.h_range[2 * b + 1] != at) return set_err(GSB_ERR_CUDA, "bucket ranges not read");
+            at += p.h_range[2 * b];
+        }
+        if (at > (unsigned long long)key.nsys) return set_err(GSB_ERR_CUDA, "bucket ranges not read");
+        for (int b = GSB_UNEVEN_BUCKETS - 1; b >= 0; --b) {
+            const unsigned long long count = p.h_range[2 * b], first = p.h_range[2 * b + 1];
+            if (!p.ordinary[b] || count == 0) continue;
+            KernelEntry* ke = p.ke[b];
+            // systems per CTA: the CTA's teams for the warp form (its size chosen at launch),
+            // the entry's fixed count otherwise
+            const int64_t spb =
+                ke->lanes ? (int64_t)p.threads[b] / ke->lanes : (int64_t)ke->systems_per_block;
+            int64_t blocks = ((int64_t)count + spb - 1) / spb;
+            if (ke->resident && blocks > (int64_t)sms * p.occ[b]) blocks = (int64_t)sms * p.occ[b];
+            Launch L{key.X, GSB_AOS, key.S, key.s_kind, key.P, GSB_AOS, p.list + first, 0,
+                     (int64_t)count, nullptr, p.work->tally, key.x_off, key.p_off, nullptr,
+                     nullptr, fault_word()};
+            ke->fn<<<(unsigned)blocks, p.threads[b], p.smem[b], p.ord>>>(key.m, key.o, L);
+            if (int rc = cuda_err(cudaGetLastError(), "kernel launch")) return rc;
+        }
+        if (int rc = cuda_err(cudaEventRecord(p.ord_done, p.ord), "event")) return rc;
+        if (int rc = cuda_err(cudaStreamWaitEvent(st, p.ord_done, 0), "stream wait")) return rc;
+    }
     unsigned long long h[7];
     if (int rc = cuda_err(cudaMemcpyAsync(h, &p.work->bad, sizeof(h), cudaMemcpyDeviceToHost, st),
                           "tally copy"))

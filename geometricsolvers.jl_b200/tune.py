@@ -11,7 +11,10 @@ fastest. A configuration is
   one-thread kernels work warp by warp and the team kernels of n = 6 and 8 hold one parameter
   row per system, so for them the CTA size is fixed;
 - the resident CTAs per SM of the bucket's persistent launch (0: as many as fit), which sets how
-  the bucket's kernel shares the GPU with the other buckets running beside it.
+  the bucket's kernel shares the GPU with the other buckets running beside it, or -1: no
+  persistent kernel but one ordinary grid, sized from the bucket's count once the bucketing has
+  run (the persistent form's work loop costs the large warp-form kernels registers and
+  instruction-cache misses).
 
 The timing batch of a size is synthetic and seeded: cubic-affine systems with A = (n+1) I +
 0.5 N(0,1) and b ~ U(-1, 1)^n from x0 = 0 (the distribution of the ragged benchmark), unless the
@@ -29,7 +32,8 @@ from .abi import UNEVEN_SIZES
 
 CANDIDATE_THREADS = {2: (1,), 3: (1,), 4: (1,), 6: (1, 2), 8: (1, 2, 4, 8), 12: (16, 32),
                      16: (16, 32), 24: (32,), 32: (32,)}
-CANDIDATE_CTAS = (0, 1, 2, 3, 4, 6, 8)
+# persistent CTAs per SM (0: as many as fit), or -1: one ordinary grid sized from the count
+CANDIDATE_CTAS = (-1, 0, 1, 2, 3, 4, 6, 8)
 # systems per CTA of the warp form, by lanes per system (CTAs of 32 to 128 threads)
 CANDIDATE_SPC = {16: (2, 4, 8), 32: (1, 2, 4)}
 

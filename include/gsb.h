@@ -346,8 +346,10 @@ GSB_API int gsb_solve_batch_host(const GsbProblem* prob, const GsbMethod* method
  * on the first call with a given set of arguments and replayed after. `table` (nullable) gives,
  * per bucket in the order of the sizes above, the threads per system (0: the default of the
  * size; 1 up to n = 8, or 2, 4, 8 lanes for n = 6 and 8 under fused arithmetic; 16 or 32 lanes
- * for n = 12 and 16; 32 for n = 24 and 32), the persistent CTAs per SM (0: as many as fit) and
- * the systems per CTA of the warp form (n >= 12: a CTA of systems_per_cta x threads_per_system
+ * for n = 12 and 16; 32 for n = 24 and 32), the persistent CTAs per SM (0: as many as fit; -1:
+ * no persistent kernel for the bucket but one ordinary grid, which the call launches from the
+ * host once the bucketing has counted the bucket's systems, beside the graph) and the systems
+ * per CTA of the warp form (n >= 12: a CTA of systems_per_cta x threads_per_system
  * lanes, a multiple of 32 and at most 128; 0: 128 lanes; the other forms take 0). The call
  * returns after the batch is solved; a size outside the set returns GSB_ERR_ARGUMENT (its
  * systems are left untouched). All pointers are device pointers.

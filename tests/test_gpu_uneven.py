@@ -98,7 +98,14 @@ def test_uneven_tables_replay_and_count_form(gsb, oracle):
     tab3[6] = (32, 0, 1)
     tab3[7] = (32, 3, 1)
     tab3[8] = (32, 0, 2)
-    for table in (None, tab, tab, tab3):  # the third call replays the graph of the second
+    # every bucket as one ordinary grid sized from its count, and a mix of the two forms
+    tab_ord = [(0, -1, 0)] * 9
+    tab_mix = list(tab3)
+    tab_mix[0] = (0, -1, 0)
+    tab_mix[4] = (0, -1, 0)
+    tab_mix[8] = (32, -1, 2)
+    for table in (None, tab, tab, tab3, tab_ord, tab_mix, tab_ord):
+        # (the third call replays the graph of the second, the last that of tab_ord)
         xg, sg = _run(gsb, m, opts, sizes, X0, P, table=table)
         assert xg.tobytes() == xo.tobytes()
         assert sg.tobytes() == so.tobytes()
@@ -147,7 +154,8 @@ def test_uneven_cta_size_rejections(gsb):
     args = (_dev(X0), None, torch.tensor(sizes, device="cuda"), _dev(P), m)
     for b, cfg in ((4, (1, 0, 2)),     # the one-thread form has a fixed CTA size
                    (8, (32, 0, 8)),    # 256 lanes: above the warp form's 128
-                   (5, (16, 0, 1))):   # 16 lanes: not a whole warp
+                   (5, (16, 0, 1)),    # 16 lanes: not a whole warp
+                   (3, (0, -2, 0))):   # CTAs per SM below -1
         tab = [(0, 0, 0)] * 9
         tab[b] = cfg
         with pytest.raises(gsb.ArgumentError):

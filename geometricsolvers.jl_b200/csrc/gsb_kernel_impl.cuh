@@ -754,10 +754,11 @@ template <class Fam, bool F> KernelEntry* trial32_entry() {
     return &e;
 }
 
-// The plain step with the static QR factor (QRFactorization, Float64, no refinement).
-template <class Fam, bool F> KernelEntry* qr_entry() {
-    static KernelEntry e{newton_kernel<Fam, F, false, false, false, true>,
-                         newton_kernel<Fam, F, false, false, true, true>,
+// The plain step with the static QR factor (QRFactorization, Float64), with or without the
+// refinement passes (Ref).
+template <class Fam, bool F, bool Ref = false> KernelEntry* qr_entry() {
+    static KernelEntry e{newton_kernel<Fam, F, false, Ref, false, true>,
+                         newton_kernel<Fam, F, false, Ref, true, true>,
                          ((SharedLen<Fam>::value + 1) / 2) * 2 + kThreads * newton_row_stride<Fam>(),
                          kThreads, {}};
     return &e;
@@ -810,9 +811,11 @@ template <class Fam> KernelEntry* pick(bool fused, bool mixed, bool refine) {
 }
 
 #define GSB_DECLARE_ENTRY(NAME) KernelEntry* entry_##NAME(bool fused, bool mixed, bool refine)
-#define GSB_DECLARE_QR(NAME) KernelEntry* qr_##NAME(bool fused)
+#define GSB_DECLARE_QR(NAME) KernelEntry* qr_##NAME(bool fused, bool refine)
 #define GSB_DEFINE_QR(NAME, ...)                                                              \
-    KernelEntry* qr_##NAME(bool fused) {                                                      \
+    KernelEntry* qr_##NAME(bool fused, bool refine) {                                         \
+        if (refine)                                                                           \
+            return fused ? qr_entry<__VA_ARGS__, true, true>() : qr_entry<__VA_ARGS__, false, true>(); \
         return fused ? qr_entry<__VA_ARGS__, true>() : qr_entry<__VA_ARGS__, false>();        \
     }
 #define GSB_DECLARE_TEAM(NAME) KernelEntry* team_##NAME(int T, bool mixed)

@@ -270,21 +270,22 @@ int tuned_team(const GsbProblem* prob, bool mixed) {
 }
 
 // The kernel of a QRFactorization call: the one-thread plain step with the static QR factor
-// (Float64, no refinement), for the square families with per-system parameter blocks.
-KernelEntry* select_qr_kernel(const GsbProblem* prob, bool fused, int T) {
+// (Float64, with or without the refinement passes), for the square families with per-system
+// parameter blocks.
+KernelEntry* select_qr_kernel(const GsbProblem* prob, bool fused, bool refine, int T) {
     if (T > 1 || shared_matrix(prob)) return nullptr;
     switch (prob->family) {
     case GSB_FAMILY_CUBIC_AFFINE:
         switch (prob->n) {
-        case 2: return qr_cubic2(fused);
-        case 3: return qr_cubic3(fused);
-        case 4: return qr_cubic4(fused);
-        case 6: return qr_cubic6(fused);
-        case 8: return qr_cubic8(fused);
+        case 2: return qr_cubic2(fused, refine);
+        case 3: return qr_cubic3(fused, refine);
+        case 4: return qr_cubic4(fused, refine);
+        case 6: return qr_cubic6(fused, refine);
+        case 8: return qr_cubic8(fused, refine);
         default: return nullptr;
         }
-    case GSB_FAMILY_HETERO6: return qr_hetero6(fused);
-    case GSB_FAMILY_COUPLED2: return qr_coupled2(fused);
+    case GSB_FAMILY_HETERO6: return qr_hetero6(fused, refine);
+    case GSB_FAMILY_COUPLED2: return qr_coupled2(fused, refine);
     default: return nullptr;
     }
 }
@@ -510,11 +511,11 @@ int select_entry(const GsbProblem* prob, const GsbMethod* method, KernelEntry** 
                                     method->reuse > 0 ? gsb::kStepReuse : gsb::kStepDogLeg,
                                     method->threads_per_system);
         } else if (method->linsolve == GSB_QR) {
-            if (mixed || method->refinement == GSB_REFINEMENT)
+            if (mixed)
                 return set_err(GSB_ERR_UNSUPPORTED,
-                               "the QRFactorization batch kernel takes a Float64 factor and no "
-                               "refinement");
-            ke = select_qr_kernel(prob, fused, method->threads_per_system);
+                               "the QRFactorization batch kernel takes a Float64 factor");
+            ke = select_qr_kernel(prob, fused, method->refinement == GSB_REFINEMENT,
+                                  method->threads_per_system);
         } else {
             if (prob->family == GSB_FAMILY_IRK3_HENON_HEILES && !prob->shared)
                 return set_err(GSB_ERR_ARGUMENT, "the step h and the tableau A are missing");

@@ -628,6 +628,15 @@ template <class Fam, int T> __host__ __device__ constexpr int warp_sys_stride() 
     return ((Fam::SP + 1) / 2) * 2 + warp_lu_doubles<Fam::N, T>();
 }
 
+// Shared memory of a batch-wide matrix at the start of a warp-form CTA (BatchParams), in doubles
+// (A with the family's column stride, rounded up to 16 bytes); 0 for a per-system block.
+template <class Fam, class = void> struct WarpSharedA {
+    static constexpr int doubles = 0;
+};
+template <class Fam> struct WarpSharedA<Fam, decltype(void(Fam::kSharedA))> {
+    static constexpr int doubles = Fam::kSharedA ? ((Fam::N * Fam::LDA + 1) / 2) * 2 : 0;
+};
+
 // Parameter k of a system to its place in the family's shared-memory layout.
 template <class Fam> struct WarpPlace {
     __device__ __forceinline__ int operator()(int k) const { return Fam::place(k); }
@@ -654,15 +663,23 @@ __global__ void __launch_bounds__(kThreads, (warp_min_blocks<Fam, T>())) warp_ke
                                  const __grid_constant__ Launch L) {
     extern __shared__ double smem[];
     constexpr int N = Fam::N, NP = Fam::NP, SS = warp_sys_stride<Fam, T>();
+    constexpr int SHA = WarpSharedA<Fam>::doubles;
     const int tid = threadIdx.x;
     const int team = tid / T;
     const int spb = (int)blockDim.x / T;
-    double* sys = smem + team * SS;
+    double* sys = smem + SHA + team * SS;
+    if constexpr (SHA > 0) {
+        // the batch's A (column-major, n x n) once per CTA, at the family's column stride
+        for (int q = tid; q < N * N; q += (int)blockDim.x)
+            smem[(q % N) + (q / N) * Fam::LDA] = __ldg(L.shared + q);
+        __syncthreads();
+    }
+    const double* fam_shared = SHA > 0 ? smem : L.shared;
     for_each_chunk<Persistent>(L, spb, [&](int64_t base, const Range& r) {
         const int64_t i = base + team;
         if (r.order == nullptr && L.p_layout == GSB_AOS && L.p_off == nullptr) {
-            stage_aos_rows<NP, SS>(smem, L.P + base * NP, r.n - base, spb, tid, (int)blockDim.x,
-                                   WarpPlace<Fam>());
+            stage_aos_rows<NP, SS>(smem + SHA, L.P + base * NP, r.n - base, spb, tid,
+                                   (int)blockDim.x, WarpPlace<Fam>());
         } else if (i < r.n) {
             const int64_t idx = r.order ? r.order[i] - L.order_base : i;
             const double* pb = param_block(L, idx, NP);
@@ -685,7 +702,7 @@ __global__ void __launch_bounds__(kThreads, (warp_min_blocks<Fam, T>())) warp_ke
         const int64_t idx = r.order ? r.order[i] - L.order_base : i;
         Team<T> tm;
         const int lane = tm.lane;
-        Fam fam{sys, L.shared};
+        Fam fam{sys, fam_shared};
         double* xb = x_block(L, idx, N);
         double xl = 0.0;
         if (lane < N) xl = L.x_layout == GSB_SOA ? L.X[(int64_t)lane * L.nsys + idx] : xb[lane];
@@ -771,10 +788,12 @@ template <class Fam, bool F, bool Mixed> KernelEntry* lm_entry() {
 }
 
 template <class Fam, int T, bool F, bool Mixed, bool PlainRef> KernelEntry* warp_entry() {
+    // (a batch-wide A, staged at the CTA's start, is a per-call form: the ragged batch, which
+    // sizes CTAs by sys_doubles, has per-system blocks only)
     static KernelEntry e{warp_kernel<Fam, T, F, Mixed, PlainRef, false>,
                          warp_kernel<Fam, T, F, Mixed, PlainRef, true>,
-                         (kThreads / T) * warp_sys_stride<Fam, T>(), kThreads / T, {}, false, T,
-                         warp_sys_stride<Fam, T>()};
+                         WarpSharedA<Fam>::doubles + (kThreads / T) * warp_sys_stride<Fam, T>(),
+                         kThreads / T, {}, false, T, warp_sys_stride<Fam, T>()};
     return &e;
 }
 

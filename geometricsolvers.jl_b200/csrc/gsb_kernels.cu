@@ -254,6 +254,10 @@ KernelEntry* warp_cubic12(bool fused, bool mixed, bool refine, int T);
 KernelEntry* warp_cubic16(bool fused, bool mixed, bool refine, int T);
 KernelEntry* warp_cubic24(bool fused, bool mixed, bool refine, int T);
 KernelEntry* warp_cubic32(bool fused, bool mixed, bool refine, int T);
+KernelEntry* warp_cubic12s(bool fused, bool mixed, bool refine, int T);
+KernelEntry* warp_cubic16s(bool fused, bool mixed, bool refine, int T);
+KernelEntry* warp_cubic24s(bool fused, bool mixed, bool refine, int T);
+KernelEntry* warp_cubic32s(bool fused, bool mixed, bool refine, int T);
 KernelEntry* warp_irk(bool fused, bool mixed, bool refine, int T);
 }  // namespace gsb
 
@@ -328,7 +332,19 @@ KernelEntry* select_trial32_kernel(const GsbProblem* prob, bool fused, int T) {
 KernelEntry* select_kernel(const GsbProblem* prob, bool fused, bool mixed, bool refine, int T) {
     if (shared_matrix(prob)) {
         // BatchParams: A shared by the batch and staged once per CTA, b per system; one thread
-        // per system (the warp and team forms read a whole (A, b) block per system)
+        // per system up to n = 8, the warp form above (the team form reads a whole (A, b)
+        // block per system)
+        if (prob->n >= 12) {
+            if (T == 0) T = prob->n <= 16 ? 16 : 32;
+            if (!(T == 32 || (T == 16 && prob->n <= 16))) return nullptr;
+            switch (prob->n) {
+            case 12: return warp_cubic12s(fused, mixed, refine, T);
+            case 16: return warp_cubic16s(fused, mixed, refine, T);
+            case 24: return warp_cubic24s(fused, mixed, refine, T);
+            case 32: return warp_cubic32s(fused, mixed, refine, T);
+            default: return nullptr;
+            }
+        }
         if (T > 1) return nullptr;
         switch (prob->n) {
         case 2: return entry_cubic2s(fused, mixed, refine);

@@ -33,20 +33,30 @@ __host__ __device__ constexpr int warp_ld(int n) { return (n % 2 == 1) ? n : n +
 // family's operations (gsb_families.cuh). `p` is the system's parameter block in shared memory:
 // A column-major with an odd column stride LDA (so that lanes reading along a row, as lanes
 // reading down a column, fall in distinct bank slots), then b.
-template <int N_> struct WarpCubic {
-    static constexpr int N = N_, NP = N_ * N_ + N_, LDA = warp_ld(N_), SP = N_ * LDA + N_;
+//
+// SA (BatchParams, src/nonlinear/batched.jl:34-47): A shared by the batch, staged once per CTA
+// into shared memory with the same odd column stride; a system's block is b alone.
+template <int N_, bool SA = false> struct WarpCubic {
+    static constexpr int N = N_, LDA = warp_ld(N_);
+    static constexpr int NP = SA ? N_ : N_ * N_ + N_, SP = SA ? N_ : N_ * LDA + N_;
+    static constexpr bool kSharedA = SA;
     static constexpr bool kDiagState = true;  // J = A except a diagonal held by the lanes
     const double* p;
-    const double* shared;  // unused: the family has no batch-wide constants
+    const double* shared;  // SA: the CTA's copy of A in shared memory; otherwise unused
     struct JState {
         double d;  // J_ii of the lane's row i
     };
     // place of parameter k (A column-major, then b) in the shared-memory block
     __host__ __device__ static constexpr int place(int k) {
+        if (SA) return k;
         return k < N * N ? (k % N) + (k / N) * LDA : N * LDA + (k - N * N);
     }
     __device__ __forceinline__ double par(int k) const { return lds(smem_addr(p) + 8u * k); }
-    __device__ __forceinline__ double A(int i, int k) const { return par(i + k * LDA); }
+    __device__ __forceinline__ double A(int i, int k) const {
+        if constexpr (SA) return lds(smem_addr(shared) + 8u * (i + k * LDA));
+        else return par(i + k * LDA);
+    }
+    __device__ __forceinline__ double bv(int r) const { return SA ? par(r) : par(N * LDA + r); }
 
     // Row i (< N) of F; every lane of the team calls it (x_j arrive by broadcast).
     template <int T>
@@ -56,7 +66,7 @@ template <int N_> struct WarpCubic {
 #pragma unroll 8
         for (int j = 1; j < N; ++j) t = __fma_rn(A(r, j), tm.bcast(xl, j), t);
         const double c = __dmul_rn(__dmul_rn(xl, xl), xl);
-        return __dsub_rn(__fma_rn(0.1, c, t), par(N * LDA + r));
+        return __dsub_rn(__fma_rn(0.1, c, t), bv(r));
     }
     // The diagonal of J at x (the rest of J is A).
     __device__ __forceinline__ double diag(int i, double xi) const {

@@ -1,0 +1,10 @@
+// Warp-form kernels of the cubic-affine family at n = 16 with one matrix A for the batch
+// (BatchParams: A staged once per CTA, b per system).
+#include "gsb_kernel_impl.cuh"
+
+namespace gsb {
+KernelEntry* warp_cubic16s(bool fused, bool mixed, bool refine, int T) {
+    if (T == 32) return pick_warp<WarpCubic<16, true>, 32>(fused, mixed, refine);
+    return pick_warp<WarpCubic<16, true>, 16>(fused, mixed, refine);
+}
+}  // namespace gsb

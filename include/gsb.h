@@ -107,7 +107,8 @@ typedef enum {
     /* F(x, p) = A x + 0.1 x.^3 - b, p = (A column-major n*n, b n); n in 1..32.
      * BatchParams form (src/nonlinear/batched.jl:34-47, parameters (shared, per_system[i])):
      * with shared = A column-major and shared_len = n*n, every system shares A and its block
-     * p is b alone (n doubles); n in {2, 3, 4, 6, 8}, one thread per system. */
+     * p is b alone (n doubles); n in {2, 3, 4, 6, 8} (one thread per system) and {12, 16,
+     * 24, 32} (the warp form, A staged once per CTA at the family's column stride). */
     GSB_FAMILY_CUBIC_AFFINE = 1,
     /* Least squares r_i = sum_j a_j exp(-b_j t_i) - y_i, i = 1..m; x = (a1, b1, a2, b2, a3, b3),
      * p = y (m values); the m abscissae t are the problem's shared constants. n = 6. */

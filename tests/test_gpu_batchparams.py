@@ -1,5 +1,6 @@
 """BatchParams(shared, per_system) (src/nonlinear/batched.jl:34-47): the cubic-affine batch with
-one matrix A shared by every system and a right-hand side b per system.
+one matrix A shared by every system and a right-hand side b per system, n = 2 … 8 (one thread per
+system) and 12 … 32 (the warp form).
 
 The device stages A once per CTA and streams only b; the oracle solves the same batch with A
 replicated into every system's (A, b) block, so the two must agree exactly as the per-system
@@ -48,9 +49,9 @@ def run_shared(gsb, prob, method, X0, A, B, options, soa=False, host=False):
 
 
 @pytest.mark.parametrize("arith", ["fused", "unfused"])
-@pytest.mark.parametrize("n", [2, 3, 4, 6, 8])
+@pytest.mark.parametrize("n", [2, 3, 4, 6, 8, 12, 16, 24, 32])
 def test_shared_matrix_parity(gsb, oracle, n, arith):
-    X0, A, B, P = shared_batch(n, 40000, n + 1.0, 10 + n)
+    X0, A, B, P = shared_batch(n, 40000 if n <= 8 else 4096, n + 1.0, 10 + n)
     prob = gsb.NonlinearProblem(gsb.CubicAffine(n))
     m = gsb.Newton(globalization=gsb.Backtracking(), arithmetic=arith)
     opts = gsb.Options(**OPTS)
@@ -60,10 +61,10 @@ def test_shared_matrix_parity(gsb, oracle, n, arith):
     assert np.all(so["code"] == 0)
 
 
-@pytest.mark.parametrize("n", [4, 8])
+@pytest.mark.parametrize("n", [4, 8, 12, 32])
 def test_shared_matrix_mixed_refinement(gsb, oracle, n):
     # FP32 factor + FP64 refinement with the shared A, on a graded spectrum that promotes
-    X0, A, B, P = shared_batch(n, 20000, 0.0, 20 + n, illcond=True)
+    X0, A, B, P = shared_batch(n, 20000 if n <= 8 else 2048, 0.0, 20 + n, illcond=True)
     prob = gsb.NonlinearProblem(gsb.CubicAffine(n))
     m = gsb.Newton(linsolve=gsb.LUFactorization("float32"), refinement=gsb.Refinement(),
                    globalization=gsb.Backtracking(), arithmetic="unfused")
@@ -88,11 +89,12 @@ def test_shared_matrix_soa_and_host(gsb, oracle):
 def test_shared_matrix_unsupported_and_mismatch(gsb):
     import torch
 
-    prob = gsb.NonlinearProblem(gsb.CubicAffine(12))
-    X = torch.zeros((64, 12), dtype=torch.float64, device="cuda")
+    # a size without a kernel of its own (n = 10) is refused with a shared A as without one
+    prob = gsb.NonlinearProblem(gsb.CubicAffine(10))
+    X = torch.zeros((64, 10), dtype=torch.float64, device="cuda")
     S = gsb.status_buffer(64)
-    A = torch.eye(12, dtype=torch.float64, device="cuda")
-    B = torch.ones((64, 12), dtype=torch.float64, device="cuda")
+    A = torch.eye(10, dtype=torch.float64, device="cuda")
+    B = torch.ones((64, 10), dtype=torch.float64, device="cuda")
     with pytest.raises(Exception, match="no batch kernel"):
         gsb.solve_batch(X, S, prob, gsb.Newton(), gsb.BatchParams(A, B))
     prob8 = gsb.NonlinearProblem(gsb.CubicAffine(8))

@@ -771,11 +771,11 @@ template <class Fam, bool F> KernelEntry* trial32_entry() {
     return &e;
 }
 
-// The plain step with the static QR factor (QRFactorization, Float64), with or without the
-// refinement passes (Ref).
-template <class Fam, bool F, bool Ref = false> KernelEntry* qr_entry() {
-    static KernelEntry e{newton_kernel<Fam, F, false, Ref, false, true>,
-                         newton_kernel<Fam, F, false, Ref, true, true>,
+// The step with the static QR factor (QRFactorization): Float64 with or without the refinement
+// passes (Ref), or the mixed step's Float32 factor (Mixed; refinement as the method says).
+template <class Fam, bool F, bool Ref = false, bool Mixed = false> KernelEntry* qr_entry() {
+    static KernelEntry e{newton_kernel<Fam, F, Mixed, Ref, false, true>,
+                         newton_kernel<Fam, F, Mixed, Ref, true, true>,
                          ((SharedLen<Fam>::value + 1) / 2) * 2 + kThreads * newton_row_stride<Fam>(),
                          kThreads, {}};
     return &e;
@@ -830,9 +830,12 @@ template <class Fam> KernelEntry* pick(bool fused, bool mixed, bool refine) {
 }
 
 #define GSB_DECLARE_ENTRY(NAME) KernelEntry* entry_##NAME(bool fused, bool mixed, bool refine)
-#define GSB_DECLARE_QR(NAME) KernelEntry* qr_##NAME(bool fused, bool refine)
+#define GSB_DECLARE_QR(NAME) KernelEntry* qr_##NAME(bool fused, bool refine, bool mixed)
 #define GSB_DEFINE_QR(NAME, ...)                                                              \
-    KernelEntry* qr_##NAME(bool fused, bool refine) {                                         \
+    KernelEntry* qr_##NAME(bool fused, bool refine, bool mixed) {                             \
+        if (mixed)                                                                            \
+            return fused ? qr_entry<__VA_ARGS__, true, false, true>()                         \
+                         : qr_entry<__VA_ARGS__, false, false, true>();                       \
         if (refine)                                                                           \
             return fused ? qr_entry<__VA_ARGS__, true, true>() : qr_entry<__VA_ARGS__, false, true>(); \
         return fused ? qr_entry<__VA_ARGS__, true>() : qr_entry<__VA_ARGS__, false>();        \

@@ -273,23 +273,23 @@ int tuned_team(const GsbProblem* prob, bool mixed) {
     return 1;
 }
 
-// The kernel of a QRFactorization call: the one-thread plain step with the static QR factor
-// (Float64, with or without the refinement passes), for the square families with per-system
-// parameter blocks.
-KernelEntry* select_qr_kernel(const GsbProblem* prob, bool fused, bool refine, int T) {
+// The kernel of a QRFactorization call: the one-thread step with the static QR factor (Float64
+// with or without the refinement passes, or the mixed step's Float32 factor), for the square
+// families with per-system parameter blocks.
+KernelEntry* select_qr_kernel(const GsbProblem* prob, bool fused, bool refine, bool mixed, int T) {
     if (T > 1 || shared_matrix(prob)) return nullptr;
     switch (prob->family) {
     case GSB_FAMILY_CUBIC_AFFINE:
         switch (prob->n) {
-        case 2: return qr_cubic2(fused, refine);
-        case 3: return qr_cubic3(fused, refine);
-        case 4: return qr_cubic4(fused, refine);
-        case 6: return qr_cubic6(fused, refine);
-        case 8: return qr_cubic8(fused, refine);
+        case 2: return qr_cubic2(fused, refine, mixed);
+        case 3: return qr_cubic3(fused, refine, mixed);
+        case 4: return qr_cubic4(fused, refine, mixed);
+        case 6: return qr_cubic6(fused, refine, mixed);
+        case 8: return qr_cubic8(fused, refine, mixed);
         default: return nullptr;
         }
-    case GSB_FAMILY_HETERO6: return qr_hetero6(fused, refine);
-    case GSB_FAMILY_COUPLED2: return qr_coupled2(fused, refine);
+    case GSB_FAMILY_HETERO6: return qr_hetero6(fused, refine, mixed);
+    case GSB_FAMILY_COUPLED2: return qr_coupled2(fused, refine, mixed);
     default: return nullptr;
     }
 }
@@ -527,10 +527,7 @@ int select_entry(const GsbProblem* prob, const GsbMethod* method, KernelEntry** 
                                     method->reuse > 0 ? gsb::kStepReuse : gsb::kStepDogLeg,
                                     method->threads_per_system);
         } else if (method->linsolve == GSB_QR) {
-            if (mixed)
-                return set_err(GSB_ERR_UNSUPPORTED,
-                               "the QRFactorization batch kernel takes a Float64 factor");
-            ke = select_qr_kernel(prob, fused, method->refinement == GSB_REFINEMENT,
+            ke = select_qr_kernel(prob, fused, method->refinement == GSB_REFINEMENT, mixed,
                                   method->threads_per_system);
         } else {
             if (prob->family == GSB_FAMILY_IRK3_HENON_HEILES && !prob->shared)

@@ -305,17 +305,25 @@ template <bool F, int N, class TF> struct LUFactor {
 // w = v / v_1 stored below the diagonal; R on and above it. The same interface as LUFactor's
 // Float64 factor (load / eliminate / ldiv), so the plain step takes either. Divisions stay
 // divisions under both arithmetics; GSB_FUSED only contracts the products and sums.
-template <bool F, int N> struct QRFactor {
+template <bool F, int N, class TF = double> struct QRFactor {
     using A_ = Arith<F>;
-    double a[N * N];
-    double tau[N];
+    static constexpr bool same = sizeof(TF) == sizeof(double);
+    // under the fused arithmetic the mixed ldiv scales by a reciprocal (see LUFactor)
+    static constexpr bool kRecip = F;
+    TF a[N * N];
+    TF tau[N];
     int info;
     int e;
+
+    __device__ __forceinline__ static TF dv(TF x, TF y) {
+        if constexpr (same) return __ddiv_rn(x, y);
+        else return __fdiv_rn(x, y);
+    }
 
     template <class Fam, class JS, int M>
     __device__ __forceinline__ void load(const Fam& fam, const JS& js, const double (&Fx)[M],
                                          double& s, double (&g)[N]) {
-        static_assert(M == N, "the square factor");
+        static_assert(M == N && same, "the square Float64 factor");
         for_each_J(fam, js, [&](int i, int k, double v) {
             a[i + k * N] = v;
             s = (i == 0 && k == 0) ? A_::mul(v, v) : A_::madd(v, v, s);
@@ -323,13 +331,29 @@ template <bool F, int N> struct QRFactor {
         });
     }
 
+    // J into the factor, factor_matrix's scaling (J / 2^e, rounded to TF), the reflections
     template <class Fam, class JS> __device__ __forceinline__ void factor(const Fam& fam, const JS& js) {
-        for_each_J(fam, js, [&](int i, int k, double v) { a[i + k * N] = v; });
-        eliminate();
+        if constexpr (same) {
+            for_each_J(fam, js, [&](int i, int k, double v) { a[i + k * N] = v; });
+            eliminate();
+        } else {
+            unsigned long long mb = 0;
+            for_each_J(fam, js, [&](int, int, double v) {
+                const unsigned long long b = FBits<double>::bits(v) & ~FBits<double>::sign_mask;
+                mb = b > mb ? b : mb;
+            });
+            const double mm = FBits<double>::from(mb);
+            e = (isfin(mm) && mm != 0.0) ? max(-1023, min(1023, jexponent(mm))) : 0;
+            for_each_J(fam, js, [&](int i, int k, double v) {
+                a[i + k * N] = TF(e == 0 ? v : scale2_in(v, -e));  // -e in [-1023, 1023]
+            });
+            reflect();
+        }
     }
 
-    // factor_matrix's scaling (J / 2^e), then the reflections (qr.jl:17-58).
+    // factor_matrix's scaling (J / 2^e) of a Float64 factor, then the reflections.
     __device__ __forceinline__ void eliminate() {
+        static_assert(same, "the Float64 factor");
         e = matrix_exponent<N * N>(a);
         if (e < 0) {
 #pragma unroll
@@ -337,76 +361,110 @@ template <bool F, int N> struct QRFactor {
         } else {
             e = 0;
         }
+        reflect();
+    }
+
+    // qr.jl:17-58: step k reflects the subcolumn, its norm taken as LAPACK's nrm2 takes it
+    // (divided by its largest |a|), in TF.
+    __device__ __forceinline__ void reflect() {
         info = 0;
 #pragma unroll
         for (int k = 0; k < N; ++k) {
-            tau[k] = 0.0;
-            // the norm of the subcolumn as LAPACK's nrm2 takes it: divided by its largest |a|
-            double amax = 0.0;
+            tau[k] = TF(0);
+            TF amax = TF(0);
 #pragma unroll
-            for (int i = k; i < N; ++i) amax = jmax(amax, fabs(a[i + k * N]));
-            double x[N];
+            for (int i = k; i < N; ++i) amax = jmax(amax, TF(fabs(a[i + k * N])));
+            TF x[N];
 #pragma unroll
             for (int i = 0; i < N; ++i)
-                x[i] = (i >= k && amax != 0.0) ? __ddiv_rn(a[i + k * N], amax) : 0.0;
-            const double sigma = __dmul_rn(amax, rnorm<F, N>(x));
-            if (sigma != 0.0) {
-                const double x1 = a[k + k * N];
-                const double ax1 = fabs(x1);
-                const double phase = x1 == 0.0 ? 1.0 : __ddiv_rn(x1, ax1);
-                const double sa = __dadd_rn(sigma, ax1);
-                const double v1 = __dmul_rn(phase, sa);
-                const double tk = __ddiv_rn(sa, sigma);
+                x[i] = (i >= k && amax != TF(0)) ? dv(a[i + k * N], amax) : TF(0);
+            const TF sigma = A_::mul(amax, rnorm<F, N>(x));
+            if (sigma != TF(0)) {
+                const TF x1 = a[k + k * N];
+                const TF ax1 = TF(fabs(x1));
+                const TF phase = x1 == TF(0) ? TF(1) : dv(x1, ax1);
+                const TF sa = A_::add(sigma, ax1);
+                const TF v1 = A_::mul(phase, sa);
+                const TF tk = dv(sa, sigma);
                 tau[k] = tk;
 #pragma unroll
-                for (int i = k + 1; i < N; ++i) a[i + k * N] = __ddiv_rn(a[i + k * N], v1);
+                for (int i = k + 1; i < N; ++i) a[i + k * N] = dv(a[i + k * N], v1);
 #pragma unroll
                 for (int j = k + 1; j < N; ++j) {
-                    double t = a[k + j * N];
+                    TF t = a[k + j * N];
 #pragma unroll
                     for (int i = k + 1; i < N; ++i) t = A_::madd(a[i + k * N], a[i + j * N], t);
-                    t = __dmul_rn(t, tk);
-                    a[k + j * N] = __dsub_rn(a[k + j * N], t);
+                    t = A_::mul(t, tk);
+                    a[k + j * N] = A_::sub(a[k + j * N], t);
 #pragma unroll
                     for (int i = k + 1; i < N; ++i) a[i + j * N] = A_::msub(a[i + k * N], t, a[i + j * N]);
                 }
-                a[k + k * N] = __dmul_rn(-phase, sigma);
+                a[k + k * N] = A_::mul(-phase, sigma);
             }
-            if (a[k + k * N] == 0.0 && info == 0) info = k + 1;
+            if (a[k + k * N] == TF(0) && info == 0) info = k + 1;
         }
     }
 
     // qr.jl:63-89: Q' r by the reflectors, then R x = Q' r.
-    __device__ __forceinline__ void backsolve(double (&x)[N]) const {
+    __device__ __forceinline__ void backsolve(TF (&x)[N]) const {
 #pragma unroll
         for (int k = 0; k < N; ++k) {
-            double t = x[k];
+            TF t = x[k];
 #pragma unroll
             for (int i = k + 1; i < N; ++i) t = A_::madd(a[i + k * N], x[i], t);
-            t = __dmul_rn(t, tau[k]);
-            x[k] = __dsub_rn(x[k], t);
+            t = A_::mul(t, tau[k]);
+            x[k] = A_::sub(x[k], t);
 #pragma unroll
             for (int i = k + 1; i < N; ++i) x[i] = A_::msub(a[i + k * N], t, x[i]);
         }
 #pragma unroll
         for (int k = N - 1; k >= 0; --k) {
-            const double xk = __ddiv_rn(x[k], a[k + k * N]);
+            const TF xk = dv(x[k], a[k + k * N]);
             x[k] = xk;
 #pragma unroll
             for (int i = 0; i < k; ++i) x[i] = A_::msub(a[i + k * N], xk, x[i]);
         }
     }
 
-    // The same-type ldiv!! (factors.jl:931-936), as LUFactor's Float64 branch.
+    // ldiv!!: same type (factors.jl:931-936), as LUFactor's Float64 branch, or mixed type
+    // (factors.jl:943-949), as its Float32 branch.
     __device__ __forceinline__ void ldiv(const double (&r)[N], double (&d)[N]) const {
-        int k = rhs_exponent<N>(r, e);
-        double x[N];
+        if constexpr (same) {
+            int k = rhs_exponent<N>(r, e);
+            double x[N];
 #pragma unroll
-        for (int i = 0; i < N; ++i) x[i] = k == 0 ? r[i] : scale2_in(r[i], -k);  // -k in [-6, 1023]
-        backsolve(x);
-        int e2 = k - e;
+            for (int i = 0; i < N; ++i) x[i] = k == 0 ? r[i] : scale2_in(r[i], -k);  // -k in [-6, 1023]
+            backsolve(x);
+            int e2 = k - e;
 #pragma unroll
-        for (int i = 0; i < N; ++i) d[i] = e2 == 0 ? x[i] : scale2_in(x[i], e2);  // e2 in [0, 1029]
+            for (int i = 0; i < N; ++i) d[i] = e2 == 0 ? x[i] : scale2_in(x[i], e2);  // e2 in [0, 1029]
+        } else {
+            double s = fabs(r[0]);
+#pragma unroll
+            for (int i = 1; i < N; ++i) s = jmax(s, fabs(r[i]));
+            if (s == 0.0) {
+#pragma unroll
+                for (int i = 0; i < N; ++i) d[i] = 0.0;
+                return;
+            }
+            TF x[N];
+#pragma unroll
+            for (int i = 0; i < N; ++i) x[i] = TF(kRecip ? __dmul_rn(r[i], __drcp_rn(s)) : __ddiv_rn(r[i], s));
+            backsolve(x);
+            int ex = 0;
+            double frac = isfin(s) ? frexp(s, &ex) : s;
+            if (!isfin(s)) ex = 0;
+#pragma unroll
+            for (int i = 0; i < N; ++i) d[i] = __dmul_rn(double(x[i]), frac);
+            const int E = ex - e;
+            if (E >= -1074 && E <= 2046) {
+#pragma unroll
+                for (int i = 0; i < N; ++i) d[i] = scale2_in(d[i], E);
+            } else {
+#pragma unroll
+                for (int i = 0; i < N; ++i) d[i] = ldexp2_slow(d[i], E);
+            }
+        }
     }
 };
 
@@ -601,8 +659,8 @@ template <bool F, int N> struct LocalLU {
 // PlainRef: the plain (TF = T) step refines its direction (Refinement with a Float64 factor), a
 // rare configuration kept in its own instantiation so the common plain step holds no refinement
 // state in registers.
-// Qr selects the static Householder QR for the plain step's factor (QRFactorization with a
-// Float64 factor), else the pivoted LU.
+// Qr selects the static Householder QR for the step's factors (QRFactorization: the plain step's
+// Float64 factor, the mixed step's Float32 factor and its Float64 fallback), else the pivoted LU.
 template <class Fam, bool F, bool Mixed, bool PlainRef = false, bool Qr = false,
           int Kind = kStepNewton>
 struct Solver {
@@ -1169,7 +1227,7 @@ struct Solver {
         bool fallback = was_promoted;
         park_x(x);
         if (!was_promoted) {
-            LUFactor<F, N, float> fac;
+            typename std::conditional<Qr, QRFactor<F, N, float>, LUFactor<F, N, float>>::type fac;
             fac.factor(fam, js);
             bool ref_failed;
             if (fac.info > 0) {
@@ -1200,7 +1258,9 @@ struct Solver {
             // the factorisation in the working precision: at every step once promoted (with the
             // refinement passes), and as the promotion of a failed Float32 step (without them)
             // the register factor for small systems; thread-local memory from n = 6 on
-            using FT = typename std::conditional<(N >= 6), LocalLU<F, N>, LUFactor<F, N, double>>::type;
+            using FT = typename std::conditional<
+                Qr, QRFactor<F, N, double>,
+                typename std::conditional<(N >= 6), LocalLU<F, N>, LUFactor<F, N, double>>::type>::type;
             FT ft;
             ft.factor(fam, js);
             if (ft.info > 0) {

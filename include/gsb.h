@@ -141,8 +141,8 @@ typedef struct {
 
 /* The factor of a Newton step: partial-pivot LU (src/linear/static/lu.jl) or Householder QR
  * without pivoting (src/linear/static/qr.jl). For a square family GSB_QR runs with a Float64
- * factor, with or without Refinement (a Float32 QR factor returns GSB_ERR_UNSUPPORTED); a
- * least-squares family's LevenbergMarquardt step takes its stacked QR. */
+ * factor (with or without Refinement) or a Float32 one (the mixed step), one thread per system,
+ * n <= 8; a least-squares family's LevenbergMarquardt step takes its stacked QR. */
 typedef enum { GSB_LU = 0, GSB_QR = 1 } GsbLinsolve;
 typedef enum { GSB_F64 = 0, GSB_F32 = 1 } GsbPrecision;
 typedef enum { GSB_NO_REFINEMENT = 0, GSB_REFINEMENT = 1 } GsbRefinementKind;

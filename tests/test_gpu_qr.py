@@ -94,16 +94,31 @@ def test_qr_refinement_parity(gsb, oracle, n, arith):
         assert np.mean(sg["code"][8192:] != so["code"][8192:]) <= 0.1
 
 
-def test_qr_refusals(gsb):
-    # the device QR step takes a Float64 factor; a Float32 QR factor is refused before a launch
-    X0, P = cubic_affine(4, 64, 5.0, 43)
-    prob = gsb.NonlinearProblem(gsb.CubicAffine(4))
+@pytest.mark.parametrize("n", [2, 3, 4, 6, 8])
+def test_qr_float32_factor_parity(gsb, oracle, n):
+    # QRFactorization(Float32) in the mixed step: the Float32 reflections, the mixed ldiv!!
+    # (factors.jl:943-949), the refinement passes and the promotion to the Float64 QR factor;
+    # well-conditioned systems and an ill-conditioned batch that promotes, bit for bit unfused
+    X0, P = cubic_affine(n, 8192, n + 1.0, 46 + n)
+    X1, P1 = cubic_affine_illcond(n, 2048, 47)
+    X0, P = np.concatenate([X0, X1]), np.concatenate([P, P1])
+    prob = gsb.NonlinearProblem(gsb.CubicAffine(n))
     opts = gsb.Options(**OPTS)
-    for m in (gsb.Newton(linsolve=gsb.QRFactorization("float32"), refinement=gsb.Refinement()),
-              gsb.Newton(linsolve=gsb.QRFactorization("float32"))):
-        with pytest.raises(gsb.ArgumentError, match="takes a Float64 factor"):
-            run_gpu(gsb, prob, m, X0, P, opts)
+    for ref in (gsb.Refinement(), gsb.NoRefinement()):
+        m = gsb.Newton(linsolve=gsb.QRFactorization("float32"), refinement=ref,
+                       globalization=gsb.Backtracking(), arithmetic="unfused")
+        xg, sg = run_gpu(gsb, prob, m, X0, P, opts)
+        xo, so = oracle.solve_batch(prob, m, X0.copy(), P, opts)
+        check_parity(xg, sg, xo, so, bitwise=True)
+    assert so["promoted"].any()
+
+
+def test_qr_refusals(gsb):
+    # the device QR step is one thread per system up to n = 8; a warp-form size is refused
+    # before a launch
     X12, P12 = cubic_affine(12, 64, 13.0, 43)
-    with pytest.raises(gsb.ArgumentError, match="no batch kernel"):
-        run_gpu(gsb, gsb.NonlinearProblem(gsb.CubicAffine(12)), gsb.Newton(
-            linsolve=gsb.QRFactorization()), X12, P12, opts)
+    opts = gsb.Options(**OPTS)
+    for lin in (gsb.QRFactorization(), gsb.QRFactorization("float32")):
+        with pytest.raises(gsb.ArgumentError, match="no batch kernel"):
+            run_gpu(gsb, gsb.NonlinearProblem(gsb.CubicAffine(12)), gsb.Newton(linsolve=lin),
+                    X12, P12, opts)
